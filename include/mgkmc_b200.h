@@ -1,0 +1,128 @@
+/*
+ * mgkmc_b200.h -- C ABI of the B200 STZ-KMC / Lippmann-Schwinger library
+ * (libmgkmc_b200.so).  Plain pointers and sizes only.
+ *
+ * The reference (mgkmc_cpp) is a header-only C++ program with no ABI; each
+ * entry point below names the reference interface it replaces.  Tensors cross
+ * the boundary as row-major D x D blocks per voxel (D = 2 or 3), voxels in the
+ * reference's order (x slowest, then y, then z), exactly the element order of
+ * the reference's std::vector<Eigen::Matrix{2,3}d> members read with (i, j).
+ * Device memory is owned by the handles.  Calls are synchronous; a handle is
+ * used by one host thread at a time (the reference objects are not re-entrant
+ * either).
+ */
+#ifndef MGKMC_B200_H
+#define MGKMC_B200_H
+
+#if defined(__GNUC__)
+#define MGK_API __attribute__((visibility("default")))
+#else
+#define MGK_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MGK_OK = 0,
+    MGK_LS_NOT_CONVERGED = 1, /* reached max_iter (the reference stops silently) */
+    MGK_BAD_SHAPE = 2,        /* grid / field sizes inconsistent */
+    MGK_OOM = 3,              /* device allocation failed */
+    MGK_DEVICE_TIMEOUT = 4,   /* a bounded device wait gave up */
+    MGK_CUDA_ERROR = 5,
+    MGK_BAD_ARG = 6,
+    MGK_UNSUPPORTED = 7,      /* option not built (e.g. fast patching) */
+    MGK_TERMINATED = 8        /* KMC instability sequence limit (kmc_solver.hpp:925-929) */
+} mgk_status;
+
+/* Text of the last error on this thread. */
+MGK_API const char* mgk_last_error(void);
+MGK_API int mgk_version(void);
+MGK_API int mgk_device_count(void);
+
+/* ---------------------------------------------------------------- LS solver
+ * Replaces spectral_solver_2d (linear_elastic_solver.hpp:146-160) and
+ * spectral_solver_3d (:431-444) together with the Green-operator setup that
+ * callers do before them (green_operator_2d/3d, :70-119 / :344-396; the
+ * operator is evaluated on the fly, so there is no Gamma argument).
+ * mgk_ls_create: dim 2 or 3; nz ignored for dim 2; plane_stress selects
+ * compute_lame_2d's plane-stress branch (dim 2 only); E, nu: N host values. */
+typedef struct mgk_ls mgk_ls;
+MGK_API mgk_status mgk_ls_create(mgk_ls** out, int dim, int nx, int ny, int nz, int plane_stress, double pixel, const double* E,
+                         const double* nu);
+/* One solve.  eps_bar: D*D prescribed mean strain.  eps_plastic: N*D*D or NULL.
+ * eps_inout: N*D*D; read as the warm start when warm != 0 (the reference's
+ * eps.size() == N branch, :181-191), written with the solution.  sig_out:
+ * N*D*D or NULL.  macro_out: 2*D*D (eps_macro then sig_macro) or NULL.
+ * iters_out: iterations run or NULL.  Returns MGK_LS_NOT_CONVERGED when the
+ * loop hit max_iter (fields are still written, like the reference). */
+MGK_API mgk_status mgk_ls_solve(mgk_ls* h, const double* eps_bar, const double* eps_plastic, double* eps_inout, int warm,
+                        double* sig_out, double* macro_out, int max_iter, double tol, int* iters_out);
+MGK_API void mgk_ls_destroy(mgk_ls* h);
+
+/* ---------------------------------------------------------------- KMC
+ * Replaces the KmcSimulation2D constructor (kmc_solver.hpp:165-182) and the
+ * KmcSimulation3D constructor (:1142-1158): the same parameters, in one struct. */
+typedef struct {
+    int dim, nx, ny, nz, M;
+    int plane_stress;         /* 2D: plane_mode == "plane_stress" */
+    int seed;
+    double gamma0, pixel;
+    /* BarrierGenerator (kmc_solver.hpp:24-33): type 0 gaussian, 1 rayleigh,
+     * 2 modified_rayleigh, 3 modified_rayleigh_with_exponential */
+    int barrier_type;
+    double bar_mean, bar_std, bar_min_cutoff, bar_max_cutoff, bar_loc, bar_scale, bar_epsilon, bar_ratio;
+    int directional;          /* softening_scheme == "directional" */
+    double softening_cap, jp, jt, neighbor_fraction, q_act_temp;
+    double temperature, strain_rate, stability_threshold, nu0;
+    int instability_kmc;      /* instability_mode == "kmc" (else "cascade") */
+    int scale_rate_by_volume, redraw_directions, redraw_barriers, use_3d_barriers;
+    int fast_patching, patch_radius, sync_interval; /* fast patching: MGK_UNSUPPORTED */
+    double ls_tol;            /* elastic_run tolerance, reference 1e-6 (:337) */
+    int ls_max_iter;          /* reference 200 */
+} mgk_kmc_params;
+
+/* run_simulation arguments (kmc_solver.hpp:721-729) plus a thermal-event cap. */
+typedef struct {
+    int n_global_steps;
+    double step_size;
+    int comp_i, comp_j;       /* driving component */
+    int n_targets;            /* mixed stress targets (Pa), sorted by (i, j) */
+    int target_i[9], target_j[9];
+    double target_v[9];
+    double mixed_tol;         /* Pa */
+    int mixed_max_iter;
+    double max_kmc_steps_pct;
+    long long max_events;     /* stop after this many thermal events; <= 0: no cap */
+    const char* output_dir;   /* NULL: no files */
+    const char* summary_filename;
+    int enable_summary_log, enable_global_log, enable_console;
+    const char* vtk_interval; /* "none" | "last" | "current" | "<int>" */
+    int vtk_elastic_only;
+} mgk_run_params;
+
+typedef struct mgk_kmc mgk_kmc;
+MGK_API mgk_status mgk_kmc_create(mgk_kmc** out, const mgk_kmc_params* p, const double* E, const double* nu);
+/* run_simulation.  trace (optional, trace_cap rows of 6 + 2*D*D doubles):
+ * [kind, a, b, total_rate, t_wait, time, eps_macro(D*D), sig_macro(D*D)],
+ * kind 0 thermal flip (a = flat mode index, b = is_instab), 1 cascade
+ * (a = batches, b = flips), 2 interval end without event (a = u1),
+ * 3 elastic step done (a = mixed-BC solves, b = elastic steps). */
+MGK_API mgk_status mgk_kmc_run(mgk_kmc* h, const mgk_run_params* rp, double* trace, long long trace_cap, long long* trace_rows);
+/* elastic_run (kmc_solver.hpp:334-339 / :1333-1338). */
+MGK_API mgk_status mgk_kmc_elastic_run(mgk_kmc* h);
+/* Public members of the reference object: 0 eps_field, 1 sig_field,
+ * 2 eps_plastic (N*D*D), 3 soft_prop (N*2), 4 last_event_time (N), 5 Q,
+ * 6 Q0 (N*M), 7 catalog (N*M*D*D), 8 prev_strain_dir (N*D*D), 9 E_field,
+ * 10 nu_field (N).  Returns the element count in *count when dst is NULL. */
+MGK_API mgk_status mgk_kmc_get_field(mgk_kmc* h, int field, double* dst, long long* count);
+/* eps_macro (D*D), sig_macro (D*D), time, then counters: thermal events,
+ * cascades, LS solves, LS iterations, elastic steps, selection margin min. */
+MGK_API mgk_status mgk_kmc_get_macro(mgk_kmc* h, double* out, int n);
+MGK_API void mgk_kmc_destroy(mgk_kmc* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGKMC_B200_H */

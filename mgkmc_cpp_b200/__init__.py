@@ -1,0 +1,309 @@
+"""mgkmc_cpp_b200 -- B200-native STZ kinetic Monte Carlo + FFT Lippmann-Schwinger solver.
+
+Python mirror of the reference's solver surface (mgkmc_cpp: kmc_solver.hpp,
+linear_elastic_solver.hpp), backed by CUDA kernels for sm_100a in
+libmgkmc_b200.so through its C ABI (include/mgkmc_b200.h):
+
+* ``spectral_solver_2d`` / ``spectral_solver_3d`` -- same arguments and results
+  as linear_elastic_solver.hpp:146-160 / :431-444 (``Gamma`` is accepted and
+  ignored: the Green operator is evaluated on the device from ``pixel``);
+  ``LsSolver`` keeps the fields resident for repeated solves.
+* ``KmcSimulation2D`` / ``KmcSimulation3D`` -- constructor arguments of
+  kmc_solver.hpp:165-182 / :1142-1158, ``run_simulation`` (:721-729),
+  ``elastic_run`` and the public fields as numpy arrays.
+* ``BarrierGenerator`` -- kmc_solver.hpp:24-33.
+
+Tensors are numpy arrays of shape (N, D, D) in the reference's voxel order.
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+from typing import Dict, Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import MgkError
+
+__all__ = ["BarrierGenerator", "LsSolver", "spectral_solver_2d", "spectral_solver_3d", "KmcSimulation2D",
+           "KmcSimulation3D", "from_config", "MgkError"]
+
+_BAR = {"gaussian": 0, "rayleigh": 1, "modified_rayleigh": 2, "modified_rayleigh_with_exponential": 3}
+
+
+@dataclasses.dataclass
+class BarrierGenerator:
+    type: str = "gaussian"
+    mean: float = 2.0
+    std_val: float = 0.6
+    min_cutoff: float = 0.1
+    max_cutoff: float = -1.0
+    loc: float = 1.0
+    scale: float = 0.5
+    epsilon: float = 0.1
+    ratio: float = 0.8
+
+
+def _as_tensors(a, N: int, D: int) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64)).reshape(N, D * D)
+    return a
+
+
+class LsSolver:
+    """Device-resident Lippmann-Schwinger solver for one grid and modulus field."""
+
+    def __init__(self, dims, E, nu, plane_mode: str = "plane_strain", pixel: float = 1.0):
+        L = _lib.lib()
+        _lib.require_device()
+        self.dims = tuple(int(d) for d in dims)
+        self.D = len(self.dims)
+        if self.D not in (2, 3):
+            raise ValueError("dims must have 2 or 3 entries")
+        self.N = int(np.prod(self.dims))
+        self._E = np.ascontiguousarray(E, dtype=np.float64).reshape(-1)
+        self._nu = np.ascontiguousarray(nu, dtype=np.float64).reshape(-1)
+        if self._E.size != self.N or self._nu.size != self.N:
+            raise ValueError("E and nu need one value per voxel")
+        h = _lib.C.c_void_p()
+        nz = self.dims[2] if self.D == 3 else 1
+        _lib.check(L.mgk_ls_create(_lib.C.byref(h), self.D, self.dims[0], self.dims[1], nz,
+                                   1 if plane_mode == "plane_stress" else 0, float(pixel), _lib.dptr(self._E),
+                                   _lib.dptr(self._nu)))
+        self._h = h
+
+    def solve(self, eps_bar, eps=None, eps_plastic=None, max_iter: int = 200, tol: float = 1e-6):
+        """Returns (eps, sig, eps_macro, sig_macro, iterations); ``eps`` given = warm start."""
+        D, N = self.D, self.N
+        eb = np.ascontiguousarray(eps_bar, dtype=np.float64).reshape(D * D)
+        warm = eps is not None and np.asarray(eps).size == N * D * D
+        e = _as_tensors(eps, N, D).copy() if warm else np.zeros((N, D * D))
+        ep = _as_tensors(eps_plastic, N, D) if eps_plastic is not None and np.asarray(eps_plastic).size else None
+        sig = np.zeros((N, D * D))
+        mac = np.zeros(2 * D * D)
+        it = _lib.C.c_int(0)
+        _lib.check(_lib.lib().mgk_ls_solve(self._h, _lib.dptr(eb), _lib.dptr(ep), _lib.dptr(e), int(warm), _lib.dptr(sig),
+                                           _lib.dptr(mac), int(max_iter), float(tol), _lib.C.byref(it)), allow=(1,))
+        return (e.reshape(N, D, D), sig.reshape(N, D, D), mac[:D * D].reshape(D, D), mac[D * D:].reshape(D, D), it.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().mgk_ls_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def spectral_solver_2d(nx, ny, E, nu, eps_bar, plane_mode="plane_strain", Gamma=None, eps=None, max_iter=200, tol=1e-6,
+                       verbose=False, eps_plastic=None, pixel=1.0):
+    """linear_elastic_solver.hpp:146-309.  Returns (eps, sig, eps_macro, sig_macro)."""
+    s = LsSolver((nx, ny), E, nu, plane_mode, pixel)
+    try:
+        e, sg, em, sm, _ = s.solve(eps_bar, eps, eps_plastic, max_iter, tol)
+    finally:
+        s.close()
+    return e, sg, em, sm
+
+
+def spectral_solver_3d(nx, ny, nz, E, nu, eps_bar, Gamma=None, eps=None, max_iter=200, tol=1e-6, verbose=False,
+                       eps_plastic=None, pixel=1.0):
+    """linear_elastic_solver.hpp:431-593.  Returns (eps, sig, eps_macro, sig_macro)."""
+    s = LsSolver((nx, ny, nz), E, nu, "plane_strain", pixel)
+    try:
+        e, sg, em, sm, _ = s.solve(eps_bar, eps, eps_plastic, max_iter, tol)
+    finally:
+        s.close()
+    return e, sg, em, sm
+
+
+_FIELDS = {"eps_field": 0, "sig_field": 1, "eps_plastic": 2, "soft_prop": 3, "last_event_time": 4, "Q": 5, "Q0": 6,
+           "catalog": 7, "prev_strain_dir": 8, "E_field": 9, "nu_field": 10}
+
+
+class _KmcBase:
+    D = 2
+
+    def _create(self, nx, ny, nz, M, gamma0, E_field, nu_field, pixel, barrier_gen, softening_scheme, softening_cap, jp,
+                jt, neighbor_softening_fraction, q_act_temp, output_dir, temperature, strain_rate, stability_threshold,
+                nu0, plane_mode, fast_patching_enabled, patch_radius, sync_interval, instability_mode, cascade_timing,
+                scale_rate_by_volume, redraw_directions, redraw_barriers, use_3d_barriers, seed, ls_tol, ls_max_iter):
+        L = _lib.lib()
+        _lib.require_device()
+        self.nx, self.ny, self.nz, self.M = nx, ny, nz, M
+        self.N = nx * ny * nz
+        self.output_dir = output_dir
+        bg = barrier_gen or BarrierGenerator()
+        if bg.type not in _BAR:
+            raise ValueError("unknown barrier type %r" % bg.type)
+        p = _lib.KmcParamsC()
+        p.dim, p.nx, p.ny, p.nz, p.M = self.D, nx, ny, nz, M
+        p.plane_stress = 1 if plane_mode == "plane_stress" else 0
+        p.seed, p.gamma0, p.pixel = int(seed), float(gamma0), float(pixel)
+        p.barrier_type = _BAR[bg.type]
+        p.bar_mean, p.bar_std, p.bar_min_cutoff, p.bar_max_cutoff = bg.mean, bg.std_val, bg.min_cutoff, bg.max_cutoff
+        p.bar_loc, p.bar_scale, p.bar_epsilon, p.bar_ratio = bg.loc, bg.scale, bg.epsilon, bg.ratio
+        p.directional = 1 if softening_scheme == "directional" else 0
+        p.softening_cap, p.jp, p.jt = softening_cap, jp, jt
+        p.neighbor_fraction, p.q_act_temp = neighbor_softening_fraction, q_act_temp
+        p.temperature, p.strain_rate, p.stability_threshold, p.nu0 = temperature, strain_rate, stability_threshold, nu0
+        p.instability_kmc = 1 if instability_mode == "kmc" else 0
+        p.scale_rate_by_volume = int(bool(scale_rate_by_volume))
+        p.redraw_directions, p.redraw_barriers = int(bool(redraw_directions)), int(bool(redraw_barriers))
+        p.use_3d_barriers = int(bool(use_3d_barriers))
+        p.fast_patching, p.patch_radius, p.sync_interval = int(bool(fast_patching_enabled)), patch_radius, sync_interval
+        p.ls_tol, p.ls_max_iter = float(ls_tol), int(ls_max_iter)
+        self._params = p
+        E = np.ascontiguousarray(E_field, dtype=np.float64).reshape(-1)
+        nu = np.ascontiguousarray(nu_field, dtype=np.float64).reshape(-1)
+        if E.size != self.N or nu.size != self.N:
+            raise ValueError("E_field and nu_field need one value per voxel")
+        h = _lib.C.c_void_p()
+        _lib.check(L.mgk_kmc_create(_lib.C.byref(h), _lib.C.byref(p), _lib.dptr(E), _lib.dptr(nu)))
+        self._h = h
+
+    def run_simulation(self, n_global_steps, step_size, component, stress_targets: Dict[Tuple[int, int], float],
+                       mixed_tol=1e-4, mixed_max_iter=50, checkpoint_interval="none", checkpoint_path="checkpoint",
+                       vtk_interval="none", vtk_elastic_only=True, track_cascades=False, enable_console_log=True,
+                       summary_filename="summary_log.txt", enable_summary_log=True, enable_global_log=True,
+                       max_kmc_steps_pct=0.3, max_events=0, trace=False, trace_cap=1 << 20):
+        """kmc_solver.hpp:721-1037.  Returns the event trace (rows of
+        [kind, a, b, total_rate, t_wait, time, eps_macro, sig_macro]) when
+        ``trace`` is true, else None.  Raises MgkError on failure; the
+        instability-limit stop (MGK_TERMINATED) returns normally."""
+        rp = _lib.RunParamsC()
+        rp.n_global_steps, rp.step_size = int(n_global_steps), float(step_size)
+        rp.comp_i, rp.comp_j = int(component[0]), int(component[1])
+        tg = sorted(stress_targets.items())
+        rp.n_targets = len(tg)
+        for k, ((i, j), v) in enumerate(tg):
+            rp.target_i[k], rp.target_j[k], rp.target_v[k] = i, j, v
+        rp.mixed_tol, rp.mixed_max_iter, rp.max_kmc_steps_pct = mixed_tol, int(mixed_max_iter), max_kmc_steps_pct
+        rp.max_events = int(max_events or 0)
+        out = self.output_dir if (enable_summary_log or enable_global_log or vtk_interval != "none") else None
+        if out:
+            os.makedirs(out, exist_ok=True)
+        rp.output_dir = out.encode() if out else None
+        rp.summary_filename = summary_filename.encode()
+        rp.enable_summary_log, rp.enable_global_log = int(bool(enable_summary_log)), int(bool(enable_global_log))
+        rp.enable_console, rp.vtk_interval, rp.vtk_elastic_only = int(bool(enable_console_log)), vtk_interval.encode(), int(vtk_elastic_only)
+        w = 6 + 2 * self.D * self.D
+        buf = np.zeros((trace_cap, w)) if trace else None
+        rows = _lib.C.c_longlong(0)
+        self.last_status = _lib.check(_lib.lib().mgk_kmc_run(self._h, _lib.C.byref(rp), _lib.dptr(buf),
+                                                             trace_cap if trace else 0, _lib.C.byref(rows)), allow=(8,))
+        if trace:
+            return buf[:min(rows.value, trace_cap)].copy()
+        return None
+
+    def elastic_run(self):
+        _lib.check(_lib.lib().mgk_kmc_elastic_run(self._h))
+
+    def _field(self, name):
+        f = _FIELDS[name]
+        n = _lib.C.c_longlong(0)
+        _lib.check(_lib.lib().mgk_kmc_get_field(self._h, f, None, _lib.C.byref(n)))
+        out = np.zeros(n.value)
+        _lib.check(_lib.lib().mgk_kmc_get_field(self._h, f, _lib.dptr(out), None))
+        D = self.D
+        if name in ("eps_field", "sig_field", "eps_plastic", "prev_strain_dir", "catalog"):
+            return out.reshape(-1, D, D)
+        if name == "soft_prop":
+            return out.reshape(-1, 2)
+        return out
+
+    def __getattr__(self, name):
+        if name in _FIELDS:
+            return self._field(name)
+        raise AttributeError(name)
+
+    def macro(self) -> np.ndarray:
+        out = np.zeros(2 * self.D * self.D + 9)
+        _lib.check(_lib.lib().mgk_kmc_get_macro(self._h, _lib.dptr(out), out.size))
+        return out
+
+    @property
+    def eps_macro(self):
+        return self.macro()[:self.D * self.D].reshape(self.D, self.D)
+
+    @property
+    def sig_macro(self):
+        DD = self.D * self.D
+        return self.macro()[DD:2 * DD].reshape(self.D, self.D)
+
+    @property
+    def time(self):
+        return float(self.macro()[2 * self.D * self.D])
+
+    @property
+    def stats(self) -> dict:
+        m = self.macro()[2 * self.D * self.D + 1:]
+        keys = ["thermal_events", "cascades", "ls_solves", "ls_iters", "elastic_steps", "min_margin", "syncs"]
+        return {k: float(v) for k, v in zip(keys, m)}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().mgk_kmc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class KmcSimulation2D(_KmcBase):
+    """kmc_solver.hpp:98-1038."""
+    D = 2
+
+    def __init__(self, nx, ny, M, gamma0, E_field, nu_field, pixel=1.0, barrier_gen=None, softening_scheme="isotropic",
+                 softening_cap=2.0, jp=10.0, jt=30.0, neighbor_softening_fraction=0.0, q_act_temp=0.37,
+                 output_dir="output", temperature=0.0, strain_rate=1.0, stability_threshold=0.0, nu0=1e13,
+                 plane_mode="plane_strain", fast_patching_enabled=False, patch_radius=5, sync_interval=100,
+                 instability_mode="cascade", cascade_timing="none", scale_rate_by_volume=True, redraw_directions=True,
+                 redraw_barriers=True, seed=42, ls_tol=1e-6, ls_max_iter=200):
+        self._create(nx, ny, 1, M, gamma0, E_field, nu_field, pixel, barrier_gen, softening_scheme, softening_cap, jp, jt,
+                     neighbor_softening_fraction, q_act_temp, output_dir, temperature, strain_rate, stability_threshold,
+                     nu0, plane_mode, fast_patching_enabled, patch_radius, sync_interval, instability_mode,
+                     cascade_timing, scale_rate_by_volume, redraw_directions, redraw_barriers, False, seed, ls_tol,
+                     ls_max_iter)
+
+
+class KmcSimulation3D(_KmcBase):
+    """kmc_solver.hpp:1040-2063."""
+    D = 3
+
+    def __init__(self, nx, ny, nz, M, gamma0, E_field, nu_field, pixel=1.0, barrier_gen=None,
+                 softening_scheme="isotropic", softening_cap=2.0, jp=10.0, jt=30.0, neighbor_softening_fraction=0.0,
+                 q_act_temp=0.37, output_dir="output", temperature=0.0, strain_rate=1.0, stability_threshold=0.0,
+                 nu0=1e13, fast_patching_enabled=False, patch_radius=5, sync_interval=100, instability_mode="cascade",
+                 cascade_timing="none", scale_rate_by_volume=True, redraw_directions=True, redraw_barriers=True,
+                 use_3d_barriers=False, seed=42, ls_tol=1e-6, ls_max_iter=200):
+        self._create(nx, ny, nz, M, gamma0, E_field, nu_field, pixel, barrier_gen, softening_scheme, softening_cap, jp,
+                     jt, neighbor_softening_fraction, q_act_temp, output_dir, temperature, strain_rate,
+                     stability_threshold, nu0, "plane_strain", fast_patching_enabled, patch_radius, sync_interval,
+                     instability_mode, cascade_timing, scale_rate_by_volume, redraw_directions, redraw_barriers,
+                     use_3d_barriers, seed, ls_tol, ls_max_iter)
+
+
+def from_config(cfg, output_dir: Optional[str] = None):
+    """Construct the simulation main.cpp:379-403 would build from a SimConfig."""
+    b = cfg.barrier
+    bg = BarrierGenerator(b.type, b.mean, b.std, b.min_cutoff, b.max_cutoff, b.loc, b.scale, b.epsilon, b.ratio)
+    kw = dict(pixel=cfg.pixel, barrier_gen=bg, softening_scheme=cfg.softening_scheme, softening_cap=cfg.softening_cap,
+              jp=cfg.jp, jt=cfg.jt, neighbor_softening_fraction=cfg.neighbor_softening_fraction,
+              q_act_temp=cfg.q_act_temp, output_dir=output_dir or cfg.output_directory, temperature=cfg.temperature,
+              strain_rate=cfg.strain_rate, stability_threshold=cfg.stability_threshold, nu0=cfg.nu0,
+              fast_patching_enabled=cfg.fast_patching, patch_radius=cfg.patch_radius,
+              sync_interval=cfg.sync_interval, instability_mode=cfg.instability_mode,
+              cascade_timing=cfg.cascade_timing, scale_rate_by_volume=cfg.scale_rate_by_volume,
+              redraw_directions=cfg.redraw_directions, redraw_barriers=cfg.redraw_barriers, seed=cfg.seed,
+              ls_tol=cfg.ls_tol, ls_max_iter=cfg.ls_max_iter)
+    if cfg.dim == 3:
+        return KmcSimulation3D(cfg.nx, cfg.ny, cfg.nz, cfg.M, cfg.gamma0, cfg.E, cfg.nu,
+                               use_3d_barriers=cfg.use_3d_barriers, **kw)
+    return KmcSimulation2D(cfg.nx, cfg.ny, cfg.M, cfg.gamma0, cfg.E, cfg.nu, plane_mode=cfg.plane_mode, **kw)

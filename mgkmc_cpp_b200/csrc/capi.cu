@@ -1,0 +1,197 @@
+// extern "C" entry points of libmgkmc_b200.so (declared in include/mgkmc_b200.h).
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/mgkmc_b200.h"
+#include "engine.cuh"
+#include "ls.cuh"
+
+namespace {
+thread_local std::string g_err;
+
+mgk_status fail(mgk_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+mgk_status from_exception(const std::exception& e) {
+    g_err = e.what();
+    if (dynamic_cast<const std::bad_alloc*>(&e)) return MGK_OOM;
+    if (dynamic_cast<const std::domain_error*>(&e)) return MGK_UNSUPPORTED;
+    if (dynamic_cast<const std::invalid_argument*>(&e)) return MGK_BAD_SHAPE;
+    if (std::strstr(e.what(), "out of memory")) return MGK_OOM;
+    return MGK_CUDA_ERROR;
+}
+}  // namespace
+
+struct mgk_ls {
+    cudaStream_t st = nullptr;
+    mgk::LsSolver* solver = nullptr;
+    int D = 2, N = 0;
+    double* d_epsp = nullptr;  // S x N
+};
+
+struct mgk_kmc {
+    mgk::KmcEngine* eng = nullptr;
+};
+
+extern "C" {
+
+const char* mgk_last_error(void) { return g_err.c_str(); }
+int mgk_version(void) { return 100; }
+int mgk_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+mgk_status mgk_ls_create(mgk_ls** out, int dim, int nx, int ny, int nz, int plane_stress, double pixel, const double* E,
+                         const double* nu) {
+    if (!out || !E || !nu) return fail(MGK_BAD_ARG, "null argument");
+    *out = nullptr;
+    if (dim != 2 && dim != 3) return fail(MGK_BAD_SHAPE, "dim must be 2 or 3");
+    if (nx < 1 || ny < 1 || (dim == 3 && nz < 1)) return fail(MGK_BAD_SHAPE, "grid sizes must be positive");
+    mgk_ls* h = new (std::nothrow) mgk_ls;
+    if (!h) return fail(MGK_OOM, "host allocation failed");
+    try {
+        if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) throw std::runtime_error("no CUDA device");
+        int dims[3] = {nx, ny, dim == 3 ? nz : 1};
+        h->solver = new mgk::LsSolver(dim, dims, plane_stress != 0, pixel, E, nu, h->st);
+        h->D = dim;
+        h->N = h->solver->N();
+    } catch (const std::exception& e) {
+        mgk_status s = from_exception(e);
+        delete h->solver;
+        if (h->st) cudaStreamDestroy(h->st);
+        delete h;
+        return s;
+    }
+    *out = h;
+    return MGK_OK;
+}
+
+mgk_status mgk_ls_solve(mgk_ls* h, const double* eps_bar, const double* eps_plastic, double* eps_inout, int warm,
+                        double* sig_out, double* macro_out, int max_iter, double tol, int* iters_out) {
+    if (!h || !eps_bar || !eps_inout) return fail(MGK_BAD_ARG, "null argument");
+    if (max_iter < 0) return fail(MGK_BAD_ARG, "max_iter < 0");
+    const int D = h->D, DD = D * D, S = D == 2 ? 3 : 6;
+    const long N = h->N;
+    try {
+        if (warm) {
+            cudaError_t e = h->solver->upload_eps(eps_inout);
+            if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+        }
+        const double* dep = nullptr;
+        if (eps_plastic) {
+            if (!h->d_epsp && cudaMalloc(&h->d_epsp, sizeof(double) * S * N) != cudaSuccess) throw std::bad_alloc();
+            std::vector<double> s((size_t)S * N);
+            for (long v = 0; v < N; ++v) {
+                const double* f = eps_plastic + v * DD;
+                if (D == 2) {
+                    s[v] = f[0];
+                    s[N + v] = f[3];
+                    s[2 * N + v] = 0.5 * (f[1] + f[2]);
+                } else {
+                    s[v] = f[0];
+                    s[N + v] = f[4];
+                    s[2 * N + v] = f[8];
+                    s[3 * N + v] = 0.5 * (f[1] + f[3]);
+                    s[4 * N + v] = 0.5 * (f[2] + f[6]);
+                    s[5 * N + v] = 0.5 * (f[5] + f[7]);
+                }
+            }
+            cudaMemcpy(h->d_epsp, s.data(), sizeof(double) * S * N, cudaMemcpyHostToDevice);
+            dep = h->d_epsp;
+        }
+        cudaError_t e = h->solver->solve(eps_bar, warm != 0, dep, max_iter, tol);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+        if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+        if (h->solver->device_error()) {
+            h->solver->clear_error();
+            return fail(MGK_DEVICE_TIMEOUT, "device wait timed out in the LS solver");
+        }
+        e = h->solver->download_eps(eps_inout);
+        if (e == cudaSuccess && sig_out) e = h->solver->download_sig(dep, sig_out);
+        if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+        int it = 0;
+        double em[9], sm[9];
+        h->solver->macro(em, sm, &it);
+        if (macro_out) {
+            std::memcpy(macro_out, em, sizeof(double) * DD);
+            std::memcpy(macro_out + DD, sm, sizeof(double) * DD);
+        }
+        if (iters_out) *iters_out = it;
+        if (it >= max_iter && max_iter > 0 && !(h->solver->host_result().diff < tol)) return MGK_LS_NOT_CONVERGED;
+    } catch (const std::exception& e) {
+        return from_exception(e);
+    }
+    return MGK_OK;
+}
+
+void mgk_ls_destroy(mgk_ls* h) {
+    if (!h) return;
+    delete h->solver;
+    if (h->d_epsp) cudaFree(h->d_epsp);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+mgk_status mgk_kmc_create(mgk_kmc** out, const mgk_kmc_params* p, const double* E, const double* nu) {
+    if (!out || !p || !E || !nu) return fail(MGK_BAD_ARG, "null argument");
+    *out = nullptr;
+    if (p->barrier_type < 0 || p->barrier_type > 3) return fail(MGK_BAD_ARG, "unknown barrier type");
+    mgk_kmc* h = new (std::nothrow) mgk_kmc;
+    if (!h) return fail(MGK_OOM, "host allocation failed");
+    try {
+        h->eng = new mgk::KmcEngine(*p, E, nu);
+    } catch (const std::exception& e) {
+        delete h;
+        return from_exception(e);
+    }
+    *out = h;
+    return MGK_OK;
+}
+
+mgk_status mgk_kmc_run(mgk_kmc* h, const mgk_run_params* rp, double* trace, long long trace_cap, long long* trace_rows) {
+    if (!h || !rp) return fail(MGK_BAD_ARG, "null argument");
+    if (rp->n_targets < 0 || rp->n_targets > 9) return fail(MGK_BAD_ARG, "n_targets out of range");
+    const int D = h->eng->D();
+    if (rp->comp_i < 0 || rp->comp_i >= D || rp->comp_j < 0 || rp->comp_j >= D) return fail(MGK_BAD_ARG, "bad driving component");
+    for (int t = 0; t < rp->n_targets; ++t)
+        if (rp->target_i[t] < 0 || rp->target_i[t] >= D || rp->target_j[t] < 0 || rp->target_j[t] >= D)
+            return fail(MGK_BAD_ARG, "bad mixed target component");
+    mgk_status s = h->eng->run(*rp, trace, trace_cap, trace_rows);
+    if (s != MGK_OK && s != MGK_TERMINATED) g_err = h->eng->last_error;
+    return s;
+}
+
+mgk_status mgk_kmc_elastic_run(mgk_kmc* h) {
+    if (!h) return fail(MGK_BAD_ARG, "null argument");
+    mgk_status s = h->eng->elastic_run();
+    if (s != MGK_OK) g_err = h->eng->last_error;
+    return s;
+}
+
+mgk_status mgk_kmc_get_field(mgk_kmc* h, int field, double* dst, long long* count) {
+    if (!h) return fail(MGK_BAD_ARG, "null argument");
+    mgk_status s = h->eng->get_field(field, dst, count);
+    if (s != MGK_OK) g_err = h->eng->last_error;
+    return s;
+}
+
+mgk_status mgk_kmc_get_macro(mgk_kmc* h, double* out, int n) {
+    if (!h || !out) return fail(MGK_BAD_ARG, "null argument");
+    h->eng->get_macro(out, n);
+    return MGK_OK;
+}
+
+void mgk_kmc_destroy(mgk_kmc* h) {
+    if (!h) return;
+    delete h->eng;
+    delete h;
+}
+
+}  // extern "C"

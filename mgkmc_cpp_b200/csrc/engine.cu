@@ -1,0 +1,766 @@
+// KmcEngine implementation: construction (kmc_solver.hpp:165-257 / :1142-1232),
+// elastic_run (:334-339), run_simulation (:721-1037 / :1735-2062) and
+// run_cascade (:464-564 / :1473-1590) over device-resident fields.
+//
+// Per thermal event the host does one stream synchronisation: the device has
+// already swept every mode (Q, rates, double-double total, unstable count);
+// the host draws u1 (and, if the event happens, u2 and the redraw values) from
+// the reference's RNG objects, uploads them with the target u2 * total, and
+// enqueues select+flip, the warm-started LS solve and the next sweep in one go.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <ctime>
+#include <limits>
+#include <stdexcept>
+#include <sys/stat.h>
+
+#include "engine.cuh"
+#include "vtu.h"
+
+namespace mgk {
+
+double wall_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+static std::string timestamp() {
+    std::time_t t = std::time(nullptr);
+    char buf[64];
+    std::strftime(buf, sizeof(buf), "%Y-%m-%d %H:%M:%S", std::localtime(&t));
+    return buf;
+}
+
+static double uniform(std::mt19937& g, double a, double b) {
+    std::uniform_real_distribution<double> d(a, b);
+    return d(g);
+}
+
+static double mod_rayleigh(const BarrierGen& b, std::mt19937& rng) {
+    double lo = std::max(0.0, b.mean - 6.0 * b.std_val);
+    double hi = b.mean + 6.0 * b.std_val;
+    double xm = (b.mean + std::sqrt(b.mean * b.mean + 4.0 * b.std_val * b.std_val)) / 2.0;
+    double cm = xm * std::exp(-((xm - b.mean) * (xm - b.mean)) / (2.0 * b.std_val * b.std_val));
+    std::uniform_real_distribution<double> dx(lo, hi), du(0.0, cm);
+    for (;;) {
+        double x = dx(rng);
+        double u = du(rng);
+        double pdf = x * std::exp(-((x - b.mean) * (x - b.mean)) / (2.0 * b.std_val * b.std_val));
+        if (u < pdf) return x;
+    }
+}
+
+double BarrierGen::generate(std::mt19937& rng) const {
+    double v = 0.0;
+    if (type == 0) {
+        std::normal_distribution<double> d(mean, std_val);
+        v = d(rng);
+    } else if (type == 1) {
+        double u = uniform(rng, 0.0, 1.0);
+        v = loc + scale * std::sqrt(-2.0 * std::log(1.0 - u));
+    } else if (type == 2) {
+        v = mod_rayleigh(*this, rng);
+    } else if (type == 3) {
+        double umix = uniform(rng, 0.0, 1.0);
+        if (umix < ratio) v = -epsilon * std::log(1.0 - uniform(rng, 0.0, 1.0));
+        else v = mod_rayleigh(*this, rng);
+    }
+    if (min_cutoff >= 0.0 && v < min_cutoff) v = min_cutoff;
+    if (max_cutoff >= 0.0 && v > max_cutoff) v = max_cutoff;
+    return v;
+}
+
+#define CK(x)                                                                                   \
+    do {                                                                                        \
+        cudaError_t e_ = (x);                                                                   \
+        if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+static const double kB = 8.617e-5;
+
+KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu) : p_(p), rng_((unsigned)p.seed) {
+    if (p.dim != 2 && p.dim != 3) throw std::invalid_argument("dim must be 2 or 3");
+    if (p.nx < 1 || p.ny < 1 || (p.dim == 3 && p.nz < 1) || p.M < 1) throw std::invalid_argument("bad grid or M");
+    if (p.fast_patching) throw std::domain_error("fast patching is not built in this library");
+    D_ = p.dim;
+    S_ = D_ == 2 ? 3 : 6;
+    C_ = (D_ == 3 && p.use_3d_barriers) ? 6 : 2;
+    M_ = p.M;
+    const long N = (long)p.nx * p.ny * (D_ == 3 ? p.nz : 1);
+    if (N * (long)M_ > 0x7fffffffL) throw std::invalid_argument("N*M exceeds 2^31");
+    N_ = (int)N;
+    NM_ = N * M_;
+    E_.assign(E, E + N);
+    nu_.assign(nu, nu + N);
+    CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    int dims[3] = {p.nx, p.ny, D_ == 3 ? p.nz : 1};
+    ls_.reset(new LsSolver(D_, dims, p.plane_stress != 0, p.pixel, E, nu, st_));
+    bar_.type = p.barrier_type;
+    bar_.mean = p.bar_mean;
+    bar_.std_val = p.bar_std;
+    bar_.min_cutoff = p.bar_min_cutoff;
+    bar_.max_cutoff = p.bar_max_cutoff;
+    bar_.loc = p.bar_loc;
+    bar_.scale = p.bar_scale;
+    bar_.epsilon = p.bar_epsilon;
+    bar_.ratio = p.bar_ratio;
+    // physics constants (kmc_solver.hpp:182, 206-214, 784-786)
+    phys_.volume = p.pixel * p.pixel * p.pixel;
+    phys_.vnu = (p.scale_rate_by_volume ? phys_.volume : 1.0) * p.nu0;
+    phys_.beta = p.temperature > 0.0 ? 1.0 / (kB * p.temperature) : std::numeric_limits<double>::infinity();
+    phys_.tau = p.temperature > 0.0 ? 1.0 / (p.nu0 * std::exp(-p.q_act_temp / (kB * p.temperature)))
+                                    : std::numeric_limits<double>::infinity();
+    phys_.softening_cap = p.softening_cap;
+    phys_.jp = p.jp;
+    phys_.jt = p.jt;
+    phys_.neigh = p.neighbor_fraction;
+    phys_.threshold = p.stability_threshold;
+    phys_.directional = p.directional;
+    phys_.kmc_mode = p.instability_kmc;
+    phys_.nx = p.nx;
+    phys_.ny = p.ny;
+    phys_.nz = D_ == 3 ? p.nz : 1;
+    // initial barriers and catalog, voxel-major / mode-minor (kmc_solver.hpp:222-240 / :1200-1215)
+    std::vector<double> Q0(NM_), cat(NM_ * C_);
+    std::normal_distribution<double> sn(0.0, 1.0);  // 2D: one object for the whole fill
+    for (long i = 0; i < NM_; ++i) {
+        Q0[i] = bar_.generate(rng_);
+        draw_mode(sn, &cat[i * C_]);
+    }
+    // device state
+    auto alloc = [&](void** ptr, size_t b) { CK(cudaMalloc(ptr, b)); };
+    dev_.D = D_;
+    dev_.S = S_;
+    dev_.C = C_;
+    dev_.M = M_;
+    dev_.N = N_;
+    dev_.NM = NM_;
+    alloc((void**)&dev_.Q0, sizeof(double) * NM_);
+    alloc((void**)&dev_.Q, sizeof(double) * NM_);
+    alloc((void**)&dev_.cat, sizeof(double) * NM_ * C_);
+    alloc((void**)&dev_.epsp_s, sizeof(double) * S_ * N);
+    alloc((void**)&dev_.soft, sizeof(double) * 2 * N);
+    alloc((void**)&dev_.last_t, sizeof(double) * N);
+    alloc((void**)&dev_.prev, sizeof(double) * C_ * N);
+    dev_.eps_s = ls_->eps_s();
+    dev_.lam = ls_->lam();
+    dev_.mu = ls_->mu();
+    CK(cudaMemcpy(dev_.Q0, Q0.data(), sizeof(double) * NM_, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dev_.cat, cat.data(), sizeof(double) * NM_ * C_, cudaMemcpyHostToDevice));
+    CK(cudaMemset(dev_.Q, 0, sizeof(double) * NM_));
+    CK(cudaMemset(dev_.epsp_s, 0, sizeof(double) * S_ * N));
+    CK(cudaMemset(dev_.soft, 0, sizeof(double) * 2 * N));
+    CK(cudaMemset(dev_.prev, 0, sizeof(double) * C_ * N));
+    std::vector<double> lt(N, -std::numeric_limits<double>::infinity());
+    CK(cudaMemcpy(dev_.last_t, lt.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+    nblk_ = kmc_sweep_blocks(NM_, items_);
+    alloc((void**)&d_blk_, sizeof(dd) * nblk_);
+    alloc((void**)&d_blk_unst_, sizeof(int) * nblk_);
+    alloc((void**)&d_blk_last_, sizeof(int) * nblk_);
+    alloc((void**)&d_status_, sizeof(KmcStatus));
+    CK(cudaMemset(d_status_, 0, sizeof(KmcStatus)));
+    CK(cudaMallocHost((void**)&h_status_, sizeof(KmcStatus)));
+    CK(cudaMallocHost((void**)&h_lsres_, sizeof(LsResult)));
+    std::memset(h_status_, 0, sizeof(KmcStatus));
+    upload_cap_ = 1 + (size_t)M_ * (C_ + 1);
+    alloc((void**)&d_upload_, sizeof(double) * upload_cap_);
+    CK(cudaMallocHost((void**)&h_upload_, sizeof(double) * upload_cap_));
+    int npow2 = 1;
+    while (npow2 < N_) npow2 <<= 1;
+    alloc((void**)&d_ckeys_, sizeof(double) * N);
+    alloc((void**)&d_cmodes_, sizeof(int) * N);
+    alloc((void**)&d_ckeys2_, sizeof(double) * npow2);
+    alloc((void**)&d_cmodes2_, sizeof(int) * npow2);
+}
+
+KmcEngine::~KmcEngine() {
+    if (st_) cudaStreamSynchronize(st_);
+    if (f_summary_) fclose(f_summary_);
+    if (f_global_) fclose(f_global_);
+    cudaFree(dev_.Q0);
+    cudaFree(dev_.Q);
+    cudaFree(dev_.cat);
+    cudaFree(dev_.epsp_s);
+    cudaFree(dev_.soft);
+    cudaFree(dev_.last_t);
+    cudaFree(dev_.prev);
+    cudaFree(d_blk_);
+    cudaFree(d_blk_unst_);
+    cudaFree(d_blk_last_);
+    cudaFree(d_status_);
+    cudaFree(d_upload_);
+    cudaFree(d_ckeys_);
+    cudaFree(d_cmodes_);
+    cudaFree(d_ckeys2_);
+    cudaFree(d_cmodes2_);
+    cudaFreeHost(h_status_);
+    cudaFreeHost(h_upload_);
+    cudaFreeHost(h_lsres_);
+    ls_.reset();
+    if (st_) cudaStreamDestroy(st_);
+}
+
+// Mode generators: the 2D catalog draw (kmc_solver.hpp:231-238, 845-850),
+// stz_mode_glass (:1042-1052, a fresh normal object per call) and
+// stz_mode_glass_3d (:1054-1074).  `sn` is the caller's persistent object (2D).
+void KmcEngine::draw_mode(std::normal_distribution<double>& sn, double* out) {
+    const double g0 = p_.gamma0;
+    if (D_ == 2) {
+        double gxx = 0.5 * g0 * sn(rng_);
+        double gxy = 0.5 * g0 * sn(rng_);
+        out[0] = gxx;
+        out[1] = gxy;
+        return;
+    }
+    if (!p_.use_3d_barriers) {
+        std::normal_distribution<double> g(0.0, 1.0);
+        double gxx = 0.5 * g0 * g(rng_);
+        double gxy = 0.5 * g0 * g(rng_);
+        out[0] = gxx;
+        out[1] = gxy;
+        return;
+    }
+    std::normal_distribution<double> g(0.0, 1.0);
+    double Mx[3][3], G[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Mx[i][j] = g(rng_);
+    double Ms[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Ms[i][j] = 0.5 * (Mx[i][j] + Mx[j][i]);
+    double tr = (Ms[0][0] + Ms[1][1]) + Ms[2][2];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) G[i][j] = Ms[i][j] - (1.0 / 3.0) * tr * (i == j ? 1.0 : 0.0);
+    double sq = 0.0;  // Frobenius norm, storage (column-major) order
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) sq += G[i][j] * G[i][j];
+    double nrm = std::sqrt(sq);
+    if (nrm < 1e-12) {
+        for (int k = 0; k < 6; ++k) out[k] = 0.0;
+        return;
+    }
+    double f = 1.0 / (std::sqrt(2.0) * nrm);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) G[i][j] = G[i][j] * f;
+    double u = uniform(rng_, 1e-15, 1.0);
+    double mag = g0 * std::sqrt(-2.0 * std::log(u));
+    out[0] = G[0][0] * mag;
+    out[1] = G[1][1] * mag;
+    out[2] = G[2][2] * mag;
+    out[3] = G[0][1] * mag;
+    out[4] = G[0][2] * mag;
+    out[5] = G[1][2] * mag;
+}
+
+// One flip's redraw values (kmc_solver.hpp:839-864 / :1854-1875), in draw order.
+void KmcEngine::gen_flip_draws(double* out) {
+    std::normal_distribution<double> sn(0.0, 1.0);
+    if (p_.redraw_directions || p_.redraw_barriers) {
+        for (int mm = 0; mm < M_; ++mm) {
+            double* r = out + (size_t)mm * (C_ + 1);
+            if (p_.redraw_directions) draw_mode(sn, r);
+            if (p_.redraw_barriers) r[C_] = bar_.generate(rng_);
+        }
+    } else {
+        draw_mode(sn, out);
+        out[C_] = bar_.generate(rng_);
+    }
+}
+
+cudaError_t KmcEngine::enqueue_elastic() {
+    cudaError_t e = ls_->solve(eps_macro_, true, dev_.epsp_s, p_.ls_max_iter, p_.ls_tol);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_lsres_, ls_->device_result(), sizeof(LsResult), cudaMemcpyDeviceToHost, st_);
+    ls_pending_ = true;
+    return e;
+}
+
+mgk_status KmcEngine::finish_elastic() {
+    if (!ls_pending_) return MGK_OK;
+    ls_pending_ = false;
+    const_cast<LsResult&>(ls_->host_result()) = *h_lsres_;
+    double em[9], sm[9];
+    int it = 0;
+    ls_->macro(em, sm, &it);
+    std::memcpy(eps_macro_, em, sizeof(double) * D_ * D_);
+    std::memcpy(sig_macro_, sm, sizeof(double) * D_ * D_);
+    stats_.ls_solves++;
+    stats_.ls_iters += it;
+    return MGK_OK;
+}
+
+cudaError_t KmcEngine::enqueue_sweep() {
+    cudaError_t e = kmc_sweep(dev_, phys_, time_, d_blk_, d_blk_unst_, d_blk_last_, nblk_, items_, d_status_, st_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_status_, d_status_, sizeof(KmcStatus), cudaMemcpyDeviceToHost, st_);
+    return e;
+}
+
+mgk_status KmcEngine::sync_status() {
+    cudaError_t e = cudaStreamSynchronize(st_);
+    stats_.syncs++;
+    if (e != cudaSuccess) {
+        last_error = cudaGetErrorString(e);
+        return MGK_CUDA_ERROR;
+    }
+    if (h_status_->err) {
+        last_error = "device selection error";
+        return MGK_CUDA_ERROR;
+    }
+    unsigned le = 0;
+    (void)le;
+    return finish_elastic();
+}
+
+mgk_status KmcEngine::elastic_run() {
+    cudaError_t e = enqueue_elastic();
+    if (e != cudaSuccess) {
+        last_error = cudaGetErrorString(e);
+        return MGK_CUDA_ERROR;
+    }
+    e = cudaStreamSynchronize(st_);
+    if (e != cudaSuccess) {
+        last_error = cudaGetErrorString(e);
+        return MGK_CUDA_ERROR;
+    }
+    if (ls_->device_error()) {
+        last_error = "device wait timed out in the LS solver";
+        return MGK_DEVICE_TIMEOUT;
+    }
+    return finish_elastic();
+}
+
+// run_cascade (kmc_solver.hpp:464-564): entered with a fresh sweep in
+// h_status_ that found unstable modes.
+mgk_status KmcEngine::run_cascade(int* steps, int* flips) {
+    int total = 0, local = 0;
+    const int limit = N_;
+    const size_t rec = (size_t)((p_.redraw_directions || p_.redraw_barriers) ? M_ : 1) * (C_ + 1);
+    while (true) {
+        if (h_status_->n_unstable == 0) break;
+        int zero = 0;
+        CK(cudaMemcpyAsync(&d_status_->n_collect, &zero, sizeof(int), cudaMemcpyHostToDevice, st_));
+        CK(kmc_cascade_collect(dev_, phys_, d_ckeys_, d_cmodes_, d_status_, st_));
+        CK(cudaMemcpyAsync(&h_status_->n_collect, &d_status_->n_collect, sizeof(int), cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+        stats_.syncs++;
+        const int n = h_status_->n_collect;
+        if (n <= 0) break;
+        // draws of the n flips in flip order (one normal object per flip)
+        const size_t need = (size_t)n * rec;
+        if (need > upload_cap_) {
+            CK(cudaStreamSynchronize(st_));
+            cudaFree(d_upload_);
+            cudaFreeHost(h_upload_);
+            upload_cap_ = need + 1;
+            CK(cudaMalloc((void**)&d_upload_, sizeof(double) * upload_cap_));
+            CK(cudaMallocHost((void**)&h_upload_, sizeof(double) * upload_cap_));
+        }
+        for (int f = 0; f < n; ++f) gen_flip_draws(h_upload_ + (size_t)f * rec);
+        CK(cudaMemcpyAsync(d_upload_, h_upload_, sizeof(double) * need, cudaMemcpyHostToDevice, st_));
+        CK(kmc_cascade_flip(dev_, phys_, d_ckeys_, d_cmodes_, n, d_ckeys2_, d_cmodes2_, time_, d_upload_,
+                            p_.redraw_directions, p_.redraw_barriers, d_status_, st_));
+        CK(enqueue_elastic());
+        total += n;
+        ++local;
+        CK(enqueue_sweep());
+        mgk_status s = sync_status();
+        if (s != MGK_OK) return s;
+        if (local > limit) break;
+    }
+    *steps = local;
+    *flips = total;
+    stats_.cascades++;
+    stats_.cascade_flips += total;
+    return MGK_OK;
+}
+
+void KmcEngine::log_line(int global_step, int elastic_steps_done, int total_kmc, const char* type, int csteps, int cflips) {
+    // do_logging (kmc_solver.hpp:606-719 / :1632-1733), same formats
+    if (!f_summary_ && !f_global_ && !console_) return;
+    const int D = D_;
+    double elapsed = wall_seconds() - t_start_;
+    double ev = eps_macro_[comp_i_ * D + comp_j_], sv = sig_macro_[comp_i_ * D + comp_j_];
+    char buf[256];
+    std::string now = timestamp();
+    snprintf(buf, sizeof(buf), "%-22s %-12.2f %-8d %-15s %-12.6f %-15.3f %-8d %-8d %-8d %-15.6e\n", now.c_str(), elapsed,
+             global_step, type, ev, sv / 1e9, total_kmc, csteps, cflips, time_);
+    if (f_summary_) fputs(buf, f_summary_);
+    if (console_) fputs(buf, stdout);
+    if (f_global_) {
+        char g[1024];
+        if (D == 2) {
+            double sig_zz = 0.0;
+            if (!p_.plane_stress) {
+                double ns = 0.0;
+                for (double v : nu_) ns += v;
+                sig_zz = (ns / nu_.size()) * (sig_macro_[0] + sig_macro_[3]);
+            }
+            snprintf(g, sizeof(g),
+                     "%-10d %-12d %-10d %-15.6f %-15.6f %-15.6f %-15.6f %-15.6f %-15.6f %-15.3f %-15.3f %-15.3f %-15.3f %-15.3f "
+                     "%-15.3f %-14d %-17d %-15.6e\n",
+                     global_step, elastic_steps_done, total_kmc, eps_macro_[0], eps_macro_[3], 0.0, eps_macro_[1], 0.0, 0.0,
+                     sig_macro_[0] / 1e9, sig_macro_[3] / 1e9, sig_zz / 1e9, sig_macro_[1] / 1e9, 0.0, 0.0, csteps, cflips, time_);
+        } else {
+            snprintf(g, sizeof(g),
+                     "%-10d %-12d %-10d %-15.6f %-15.6f %-15.6f %-15.6f %-15.6f %-15.6f %-15.3f %-15.3f %-15.3f %-15.3f %-15.3f "
+                     "%-15.3f %-14d %-17d %-15.6e\n",
+                     global_step, elastic_steps_done, total_kmc, eps_macro_[0], eps_macro_[4], eps_macro_[8], eps_macro_[1],
+                     eps_macro_[2], eps_macro_[5], sig_macro_[0] / 1e9, sig_macro_[4] / 1e9, sig_macro_[8] / 1e9,
+                     sig_macro_[1] / 1e9, sig_macro_[2] / 1e9, sig_macro_[5] / 1e9, csteps, cflips, time_);
+        }
+        fputs(g, f_global_);
+    }
+}
+
+void KmcEngine::export_vtu(const std::string& name) {
+    const int D = D_;
+    const size_t N = N_;
+    std::vector<double> eps(N * D * D), sig(N * D * D), epsp(N * D * D), soft(2 * N);
+    long long cnt;
+    get_field(0, eps.data(), &cnt);
+    get_field(1, sig.data(), &cnt);
+    get_field(2, epsp.data(), &cnt);
+    get_field(3, soft.data(), &cnt);
+    write_vtu_fields(name, D, p_.nx, p_.ny, D == 3 ? p_.nz : 1, eps.data(), sig.data(), E_.data(), nu_.data(), p_.pixel,
+                     epsp.data(), soft.data());
+}
+
+void KmcEngine::maybe_vtk(int global_step, int elastic_steps_done, const char* type, bool init) {
+    if (outdir_.empty() || vtk_interval_ == "none") return;
+    std::string name;
+    if (init) {
+        if (vtk_interval_ == "last") return;
+        if (vtk_interval_ == "current") name = outdir_ + "/step.vtu";
+        else {
+            char b[64];
+            snprintf(b, sizeof(b), "/vtk_step_%06d.vtu", 0);
+            name = outdir_ + b;
+        }
+    } else if (vtk_interval_ == "current") {
+        name = outdir_ + "/step.vtu";
+    } else {
+        int interval = 0;
+        try {
+            interval = std::stoi(vtk_interval_);
+        } catch (...) {
+            return;
+        }
+        if (interval <= 0) return;
+        bool ok = vtk_elastic_only_ ? (std::strcmp(type, "ELASTIC") == 0 && elastic_steps_done % interval == 0)
+                                    : (global_step % interval == 0);
+        if (!ok) return;
+        char b[64];
+        snprintf(b, sizeof(b), "/vtk_step_%06d.vtu", global_step);
+        name = outdir_ + b;
+    }
+    export_vtu(name);
+}
+
+mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap, long long* rows_out) {
+    const int D = D_, DD = D * D;
+    long long rows = 0;
+    auto push = [&](double kind, double a, double b, double R, double tw) {
+        if (trace && rows < cap) {
+            double* r = trace + rows * (6 + 2 * DD);
+            r[0] = kind;
+            r[1] = a;
+            r[2] = b;
+            r[3] = R;
+            r[4] = tw;
+            r[5] = time_;
+            for (int c = 0; c < DD; ++c) {
+                r[6 + c] = eps_macro_[c];
+                r[6 + DD + c] = sig_macro_[c];
+            }
+        }
+        ++rows;
+    };
+    comp_i_ = rp.comp_i;
+    comp_j_ = rp.comp_j;
+    console_ = rp.enable_console != 0;
+    vtk_interval_ = rp.vtk_interval ? rp.vtk_interval : "none";
+    vtk_elastic_only_ = rp.vtk_elastic_only != 0;
+    outdir_.clear();
+    if (rp.output_dir && rp.output_dir[0]) {
+        outdir_ = rp.output_dir;
+        mkdir(outdir_.c_str(), 0755);
+        const std::string header =
+            "Timestamp              Elapsed(s)   Step     Type            Eps_xx       Sig_xx(GPa)     KMC      Cascade  Flips    SimTime(s)\n";
+        if (rp.enable_summary_log) {
+            f_summary_ = fopen((outdir_ + "/" + (rp.summary_filename ? rp.summary_filename : "summary_log.txt")).c_str(), "w");
+            if (f_summary_) {
+                fputs(header.c_str(), f_summary_);
+                fputs((std::string(header.size() - 1, '-') + "\n").c_str(), f_summary_);
+            }
+        }
+        if (rp.enable_global_log) {
+            f_global_ = fopen((outdir_ + "/global_log.txt").c_str(), "w");
+            if (f_global_)
+                fprintf(f_global_, "%-10s %-12s %-10s %-15s %-15s %-15s %-15s %-15s %-15s %-15s %-15s %-15s %-15s %-15s %-15s %-14s %-17s SimTime(s)\n",
+                        "GlobalStep", "ElasticStep", "KMCStep", "Eps_xx", "Eps_yy", "Eps_zz", "Eps_xy", "Eps_xz", "Eps_yz",
+                        "Sig_xx(GPa)", "Sig_yy(GPa)", "Sig_zz(GPa)", "Sig_xy(GPa)", "Sig_xz(GPa)", "Sig_yz(GPa)", "CascadeSteps",
+                        "TotalCascadeFlips");
+        }
+    }
+    t_start_ = wall_seconds();
+    auto close_logs = [&]() {
+        if (f_summary_) fclose(f_summary_);
+        if (f_global_) fclose(f_global_);
+        f_summary_ = f_global_ = nullptr;
+    };
+    int elastic_done = 0, total_kmc = 0, step = 1, seq_instab = 0;
+    const int max_seq = (int)(rp.max_kmc_steps_pct * (double)N_);
+    mgk_status s;
+    try {
+        CK(enqueue_elastic());
+        CK(enqueue_sweep());
+        s = sync_status();
+        if (s != MGK_OK) return s;
+        if (console_) {
+            fputs("Timestamp              Elapsed(s)   Step     Type            Eps_xx       Sig_xx(GPa)     KMC      Cascade  Flips    SimTime(s)\n", stdout);
+            fputs("-----------------------------------------------------------------------------------------------------------------------------\n", stdout);
+        }
+        maybe_vtk(0, 0, "INIT", true);
+        const int ci = rp.comp_i * D + rp.comp_j;
+        const double dt_step = std::fabs(rp.step_size) / p_.strain_rate;
+        double remaining = 0.0;
+        std::uniform_real_distribution<double> U(0.0, 1.0);
+        bool stop = false;
+        while (elastic_done < rp.n_global_steps && !stop) {
+            remaining += dt_step;
+            while (remaining > 0.0) {
+                // h_status_ holds the sweep of the current state (update_barriers)
+                if (!p_.instability_kmc && h_status_->n_unstable > 0) {
+                    int cs = 0, cf = 0;
+                    s = run_cascade(&cs, &cf);
+                    if (s != MGK_OK) {
+                        close_logs();
+                        return s;
+                    }
+                    if (cf > 0) {
+                        log_line(step, elastic_done, total_kmc, "CASCADE", cs, cf);
+                        maybe_vtk(step, elastic_done, "CASCADE", false);
+                        push(1, cs, cf, 0, 0);
+                        step++;
+                    }
+                    continue;
+                }
+                const double R = h_status_->total_hi + h_status_->total_lo;
+                if (R > 0.0) {
+                    const double u1 = U(rng_);
+                    const double tw = -std::log(u1) / R;
+                    if (tw < remaining) {
+                        time_ += tw;
+                        eps_macro_[ci] += 1.0 * (p_.strain_rate * tw);
+                        remaining -= tw;
+                        h_upload_[0] = U(rng_) * R;
+                        gen_flip_draws(h_upload_ + 1);
+                        const size_t nup = 1 + (size_t)((p_.redraw_directions || p_.redraw_barriers) ? M_ : 1) * (C_ + 1);
+                        CK(cudaMemcpyAsync(d_upload_, h_upload_, sizeof(double) * nup, cudaMemcpyHostToDevice, st_));
+                        CK(kmc_select_flip(dev_, phys_, d_blk_, d_blk_last_, nblk_, items_, d_upload_, time_, d_upload_ + 1,
+                                           p_.redraw_directions, p_.redraw_barriers, d_status_, st_));
+                        CK(enqueue_elastic());
+                        CK(enqueue_sweep());
+                        s = sync_status();
+                        if (s != MGK_OK) {
+                            close_logs();
+                            return s;
+                        }
+                        stats_.thermal_events++;
+                        if (h_status_->margin < stats_.min_margin) stats_.min_margin = h_status_->margin;
+                        const bool instab = h_status_->is_instab != 0;
+                        seq_instab = instab ? seq_instab + 1 : 0;
+                        if (seq_instab > max_seq) {
+                            if (console_)
+                                printf("\n[TERMINATE] KMC instability sequence limit reached! %d steps.\n", seq_instab);
+                            push(0, h_status_->selected, 1, R, tw);
+                            close_logs();
+                            if (rows_out) *rows_out = rows;
+                            return MGK_TERMINATED;
+                        }
+                        log_line(step, elastic_done, total_kmc, instab ? "KMC_INSTAB" : "KMC", 0, 1);
+                        maybe_vtk(step, elastic_done, instab ? "KMC_INSTAB" : "KMC", false);
+                        push(0, h_status_->selected, instab ? 1 : 0, R, tw);
+                        total_kmc++;
+                        step++;
+                        if (rp.max_events > 0 && stats_.thermal_events >= rp.max_events) {
+                            stop = true;
+                            break;
+                        }
+                        continue;
+                    }
+                    push(2, u1, 0, R, tw);
+                }
+                eps_macro_[ci] += 1.0 * (p_.strain_rate * remaining);
+                time_ += remaining;
+                remaining = 0.0;
+            }
+            if (stop) break;
+            // mixed boundary conditions (kmc_solver.hpp:955-987)
+            double Es = 0.0, ns = 0.0;
+            for (double v : E_) Es += v;
+            for (double v : nu_) ns += v;
+            const double Ea = Es / E_.size(), na = ns / nu_.size();
+            int solves = 0;
+            for (int it = 0; it < rp.mixed_max_iter; ++it) {
+                s = elastic_run();
+                if (s != MGK_OK) {
+                    close_logs();
+                    return s;
+                }
+                ++solves;
+                double err[9] = {0}, emax = 0.0;
+                for (int t = 0; t < rp.n_targets; ++t) {
+                    const int k = rp.target_i[t] * D + rp.target_j[t];
+                    const double e = rp.target_v[t] - sig_macro_[k];
+                    err[k] = e;
+                    emax = std::max(emax, std::fabs(e));
+                }
+                if (emax < rp.mixed_tol) break;
+                double tr = 0.0;
+                for (int a = 0; a < D; ++a) tr += err[a * D + a];
+                for (int t = 0; t < rp.n_targets; ++t) {
+                    const int a = rp.target_i[t], b = rp.target_j[t], k = a * D + b;
+                    eps_macro_[k] += (err[k] - na * tr * (a == b ? 1.0 : 0.0)) / Ea;
+                }
+            }
+            elastic_done++;
+            stats_.elastic_steps++;
+            log_line(step, elastic_done, total_kmc, "ELASTIC", 0, 0);
+            maybe_vtk(step, elastic_done, "ELASTIC", false);
+            push(3, solves, elastic_done, 0, 0);
+            step++;
+            // the state changed (eps_macro, LS): fresh sweep for the next interval
+            CK(enqueue_sweep());
+            s = sync_status();
+            if (s != MGK_OK) {
+                close_logs();
+                return s;
+            }
+        }
+        // final VTK (kmc_solver.hpp:998-1016)
+        if (!outdir_.empty() && vtk_interval_ != "none") {
+            bool fin = vtk_interval_ == "last";
+            if (!fin) {
+                try {
+                    int interval = std::stoi(vtk_interval_);
+                    fin = interval > 0 && (step - 1) % interval != 0;
+                } catch (...) {
+                }
+            }
+            if (fin) {
+                char b[64];
+                snprintf(b, sizeof(b), "/vtk_step_%06d_final.vtu", step - 1);
+                export_vtu(outdir_ + b);
+            }
+        }
+        double dur = wall_seconds() - t_start_;
+        int h = (int)(dur / 3600.0), m = (int)((dur - h * 3600.0) / 60.0);
+        double sec = dur - h * 3600.0 - m * 60.0;
+        char fin[256];
+        snprintf(fin, sizeof(fin), "\nSimulation Finish Time: %s\nTotal Duration: %.2f seconds (%dh %02dm %02ds)\n",
+                 timestamp().c_str(), dur, h, m, (int)sec);
+        if (f_summary_) fputs(fin, f_summary_);
+        if (console_) fputs(fin, stdout);
+    } catch (const std::exception& ex) {
+        last_error = ex.what();
+        close_logs();
+        return MGK_CUDA_ERROR;
+    }
+    close_logs();
+    if (rows_out) *rows_out = rows;
+    return MGK_OK;
+}
+
+mgk_status KmcEngine::get_field(int field, double* dst, long long* count) {
+    const int D = D_, DD = D * D;
+    const long N = N_;
+    long long n = 0;
+    switch (field) {
+        case 0: case 1: case 2: case 8: n = N * DD; break;
+        case 3: n = 2 * N; break;
+        case 4: case 9: case 10: n = N; break;
+        case 5: case 6: n = NM_; break;
+        case 7: n = NM_ * DD; break;
+        default: last_error = "unknown field"; return MGK_BAD_ARG;
+    }
+    if (count) *count = n;
+    if (!dst) return MGK_OK;
+    cudaStreamSynchronize(st_);
+    auto sym_to_full = [&](const std::vector<double>& s, int ncomp_is_cat, long cnt, double* out) {
+        // s: per-item C (catalog) or S (sym) values, item-major for catalog, comp-major for fields
+        (void)ncomp_is_cat;
+        (void)cnt;
+        (void)s;
+        (void)out;
+    };
+    (void)sym_to_full;
+    auto cat_full = [&](const double* c, double* o) {
+        for (int k = 0; k < DD; ++k) o[k] = 0.0;
+        if (C_ == 2) {
+            o[0] = c[0];
+            o[D + 1] = -c[0];
+            o[1] = c[1];
+            o[D] = c[1];
+        } else {
+            o[0] = c[0]; o[4] = c[1]; o[8] = c[2];
+            o[1] = o[3] = c[3];
+            o[2] = o[6] = c[4];
+            o[5] = o[7] = c[5];
+        }
+    };
+    try {
+        if (field == 0) {
+            CK(ls_->download_eps(dst));
+        } else if (field == 1) {
+            CK(ls_->download_sig(dev_.epsp_s, dst));
+        } else if (field == 2) {
+            std::vector<double> s((size_t)S_ * N);
+            CK(cudaMemcpy(s.data(), dev_.epsp_s, sizeof(double) * S_ * N, cudaMemcpyDeviceToHost));
+            static const int map2[4] = {0, 2, 2, 1};
+            static const int map3[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+            for (long v = 0; v < N; ++v)
+                for (int k = 0; k < DD; ++k) dst[v * DD + k] = s[(size_t)(D == 2 ? map2[k] : map3[k]) * N + v];
+        } else if (field == 3) {
+            CK(cudaMemcpy(dst, dev_.soft, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost));
+        } else if (field == 4) {
+            CK(cudaMemcpy(dst, dev_.last_t, sizeof(double) * N, cudaMemcpyDeviceToHost));
+        } else if (field == 5) {
+            CK(cudaMemcpy(dst, dev_.Q, sizeof(double) * NM_, cudaMemcpyDeviceToHost));
+        } else if (field == 6) {
+            CK(cudaMemcpy(dst, dev_.Q0, sizeof(double) * NM_, cudaMemcpyDeviceToHost));
+        } else if (field == 7) {
+            std::vector<double> c((size_t)NM_ * C_);
+            CK(cudaMemcpy(c.data(), dev_.cat, sizeof(double) * NM_ * C_, cudaMemcpyDeviceToHost));
+            for (long i = 0; i < NM_; ++i) cat_full(&c[(size_t)i * C_], dst + i * DD);
+        } else if (field == 8) {
+            std::vector<double> c((size_t)N * C_);
+            CK(cudaMemcpy(c.data(), dev_.prev, sizeof(double) * N * C_, cudaMemcpyDeviceToHost));
+            for (long v = 0; v < N; ++v) cat_full(&c[(size_t)v * C_], dst + v * DD);
+        } else if (field == 9) {
+            std::memcpy(dst, E_.data(), sizeof(double) * N);
+        } else if (field == 10) {
+            std::memcpy(dst, nu_.data(), sizeof(double) * N);
+        }
+    } catch (const std::exception& ex) {
+        last_error = ex.what();
+        return MGK_CUDA_ERROR;
+    }
+    return MGK_OK;
+}
+
+void KmcEngine::get_macro(double* out, int n) const {
+    const int DD = D_ * D_;
+    std::vector<double> v;
+    for (int c = 0; c < DD; ++c) v.push_back(eps_macro_[c]);
+    for (int c = 0; c < DD; ++c) v.push_back(sig_macro_[c]);
+    v.push_back(time_);
+    v.push_back((double)stats_.thermal_events);
+    v.push_back((double)stats_.cascades);
+    v.push_back((double)stats_.ls_solves);
+    v.push_back((double)stats_.ls_iters);
+    v.push_back((double)stats_.elastic_steps);
+    v.push_back(stats_.min_margin);
+    v.push_back((double)stats_.syncs);
+    for (int i = 0; i < n && i < (int)v.size(); ++i) out[i] = v[i];
+}
+
+}  // namespace mgk

@@ -1,0 +1,74 @@
+// Device kernels of the STZ kinetic Monte Carlo step (see kmc_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace mgk {
+
+// Per-voxel / per-mode state on the device.  Catalog modes are stored with
+// C = 2 values (gxx, gxy: the deviatoric 2x2 mode [[gxx, gxy], [gxy, -gxx]],
+// embedded in the xy block in 3D) or C = 6 symmetric components
+// {xx, yy, zz, xy, xz, yz} (random 3D modes).
+struct KmcDevState {
+    int D, S, C, M, N;
+    long NM;
+    double* Q0;       // NM
+    double* Q;        // NM (written by the sweep)
+    double* cat;      // NM * C
+    double* epsp_s;   // S * N
+    double* soft;     // 2 * N: g_p, g_t
+    double* last_t;   // N
+    double* prev;     // N * C: catalog entry of the last flip per voxel
+    const double* eps_s;  // S * N (owned by the LS solver)
+    const double* lam;    // N
+    const double* mu;     // N
+};
+
+struct KmcPhys {
+    double volume;        // pixel^3 (work term)
+    double vnu;           // eff_volume * nu0
+    double beta;          // 1 / (kB T), +inf at T = 0
+    double tau;           // softening decay time, +inf at T = 0
+    double softening_cap;
+    double jp, jt, neigh;
+    double threshold;     // stability threshold
+    int directional;      // softening_scheme == "directional"
+    int kmc_mode;         // instability_mode == "kmc" (rates for all modes)
+    int nx, ny, nz;
+};
+
+struct KmcStatus {
+    double total_hi, total_lo;  // sum of rates (double-double)
+    int n_unstable;             // modes with Q < threshold
+    int last_included;          // highest mode index with a rate entry, -1 if none
+    int selected;               // last selected mode index
+    int is_instab;              // Q[selected] <= threshold
+    double margin;              // relative distance of the target to the nearest prefix boundary
+    int n_collect;              // cascade: unstable voxels collected
+    unsigned err;
+    unsigned ticket;            // internal: last-block-done counter
+    int pad;
+};
+
+// Enqueue helpers (all asynchronous on `st`).
+cudaError_t kmc_sweep(const KmcDevState& s, const KmcPhys& p, double time, dd* blk, int* blk_unst, int* blk_last, int nblk,
+                      int items, KmcStatus* status, cudaStream_t st);
+int kmc_sweep_blocks(long NM, int items);
+// Select the first mode whose rate prefix reaches `target` (from the host:
+// u2 * total) and apply the flip at simulation time `time` with the M redraw
+// records in `draws` (M x (C + 1): catalog values then Q0; `redraw_dir`,
+// `redraw_bar` say which parts are replaced).
+cudaError_t kmc_select_flip(const KmcDevState& s, const KmcPhys& p, const dd* blk, const int* blk_last, int nblk, int items,
+                            const double* target_dev, double time, const double* draws, int redraw_dir, int redraw_bar,
+                            KmcStatus* status, cudaStream_t st);
+// Cascade: per-voxel most unstable mode -> list (Q, mode), count in status->n_collect.
+cudaError_t kmc_cascade_collect(const KmcDevState& s, const KmcPhys& p, double* keys, int* modes, KmcStatus* status,
+                                cudaStream_t st);
+// Sort the collected list by (Q, mode) and apply the flips in that order with
+// draw block k for the k-th flip.
+cudaError_t kmc_cascade_flip(const KmcDevState& s, const KmcPhys& p, double* keys, int* modes, int n, double* tmp_keys,
+                             int* tmp_modes, double time, const double* draws, int redraw_dir, int redraw_bar,
+                             KmcStatus* status, cudaStream_t st);
+
+}  // namespace mgk

@@ -1,0 +1,727 @@
+// Lippmann-Schwinger solver kernels and host driver (see ls.cuh for the design).
+//
+// Reference semantics kept (linear_elastic_solver.hpp:146-309 / :431-593):
+//  * warm start shifts the field mean to eps_bar (:181-191), cold start fills it;
+//  * one iteration: sigma = C:(eps - eps_p); tau = sigma - C0:eps; eps_new =
+//    eps_bar - IFFT(Gamma0 : FFT(tau)); diff = |eps_new - eps| / (|eps| + 1e-20)
+//    (Frobenius norms over all voxels, full tensors); stop when diff < tol;
+//  * lam0, mu0 from the voxel means of E and nu (:162-178); Gamma0 closed form
+//    with A = 1/(4 mu0), B = (lam0+mu0)/(mu0 (lam0+2 mu0)), Gamma(0) = 0 (:70-119).
+// Differences in arithmetic only:
+//  * the reference transforms every component with complex FFTs and keeps the
+//    real part of the inverse; on even-length axes its Gamma is not Hermitian on
+//    the Nyquist planes, so the kept real part equals the inverse transform of
+//    the Hermitian average 0.5*(Gamma(q) + Gamma(q with the Nyquist components
+//    negated)) : tau_hat.  This solver applies exactly that average on Nyquist
+//    bins and uses real-to-complex transforms;
+//  * the mean of the fluctuation field is zero by construction (Gamma(0) = 0),
+//    so the reference's mean subtraction (:263-271) only removes rounding noise
+//    and is not repeated here;
+//  * the symmetric part of eps is stored; the antisymmetric part is uniform
+//    (it only ever comes from eps_bar) and is carried as three scalars.
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#include "ls.cuh"
+
+namespace mgk {
+
+namespace {
+
+__host__ __device__ inline int n_sym(int D) { return D == 2 ? 3 : 6; }
+
+// symmetric component index of tensor entry (i, j): 2D {xx, yy, xy},
+// 3D {xx, yy, zz, xy, xz, yz}
+__host__ __device__ inline int sym_idx(int D, int i, int j) {
+    if (i == j) return i;
+    if (D == 2) return 2;
+    int a = i < j ? i : j, b = i < j ? j : i;
+    return (a == 0 && b == 1) ? 3 : (a == 0 ? 4 : 5);
+}
+
+MGK_DEV double kfreq(int i, int n, double pixel) {
+    // 2*pi*fftfreq(n, pixel)[i], as init_gamma builds it (kmc_solver.hpp:259-274)
+    const int lim = (n + 1) / 2;
+    const double f = (i < lim) ? (double)i / (n * pixel) : (double)(i - n) / (n * pixel);
+    return 2.0 * 3.14159265358979323846 * f;
+}
+
+// eps_hat = -Gamma0(q) : tau_hat for the symmetric components (in place).
+template <int D, typename T>
+MGK_DEV void green_q(const double* qd, cplx<T>* t, double inv2mu0, double bcoef) {
+    constexpr int S = D == 2 ? 3 : 6;
+    T q[D];
+    T k2 = 0;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        q[i] = (T)qd[i];
+        k2 += q[i] * q[i];
+    }
+    if (k2 == T(0)) {
+#pragma unroll
+        for (int c = 0; c < S; ++c) t[c] = {T(0), T(0)};
+        return;
+    }
+    cplx<T> v[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        cplx<T> acc = {T(0), T(0)};
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            const cplx<T> tij = t[sym_idx(D, i, j)];
+            acc.x += tij.x * q[j];
+            acc.y += tij.y * q[j];
+        }
+        v[i] = acc;
+    }
+    cplx<T> qv = {T(0), T(0)};
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        qv.x += q[i] * v[i].x;
+        qv.y += q[i] * v[i].y;
+    }
+    const T a = T(inv2mu0) / k2, b = T(bcoef) / (k2 * k2);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = i; j < D; ++j) {
+            const int c = sym_idx(D, i, j);
+            const T qq = b * q[i] * q[j];
+            t[c].x = -(a * (q[j] * v[i].x + q[i] * v[j].x) - qq * qv.x);
+            t[c].y = -(a * (q[j] * v[i].y + q[i] * v[j].y) - qq * qv.y);
+        }
+}
+
+// Hermitian-averaged Green application (see the header comment): averages over
+// the sign of every Nyquist component of q.
+template <int D, typename T>
+MGK_DEV void green_apply(const double* q, const bool* nyq, cplx<T>* t, double inv2mu0, double bcoef) {
+    constexpr int S = D == 2 ? 3 : 6;
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < D; ++i) any |= nyq[i];
+    if (!any) {
+        green_q<D, T>(q, t, inv2mu0, bcoef);
+        return;
+    }
+    cplx<T> t0[S], t1[S];
+    double q1[D];
+#pragma unroll
+    for (int c = 0; c < S; ++c) t0[c] = t1[c] = t[c];
+#pragma unroll
+    for (int i = 0; i < D; ++i) q1[i] = nyq[i] ? -q[i] : q[i];
+    green_q<D, T>(q, t0, inv2mu0, bcoef);
+    green_q<D, T>(q1, t1, inv2mu0, bcoef);
+#pragma unroll
+    for (int c = 0; c < S; ++c) t[c] = {T(0.5) * (t0[c].x + t1[c].x), T(0.5) * (t0[c].y + t1[c].y)};
+}
+
+// Row pass along the contiguous axis.  MODE 0 (prologue): set the field (warm
+// shift or fill), build tau, forward transform.  MODE 1 (iteration): inverse
+// transform of the Green-filtered spectrum, strain update with norms and
+// macro sums, then tau of the new field and its forward transform.
+template <int D, typename T, int MODE>
+MGK_DEV void row_pass(const LsArgs& a, cplx<T>* buf0, cplx<T>* buf1, double* part, const double* shift) {
+    constexpr int S = D == 2 ? 3 : 6;
+    const int n = a.nr, nh = a.nh, N = a.N;
+    cplx<T>* spec = reinterpret_cast<cplx<T>*>(a.spec);
+    const long cs = (long)a.nrows * nh;
+    const int nchunks = (a.nrows + a.rpb - 1) / a.rpb;
+    const FftAxis& ax = a.ax[D - 1];
+    for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        const int row0 = ch * a.rpb;
+        const int rows = min(a.rpb, a.nrows - row0);
+        const int L = rows * S;        // real lines in this chunk
+        const int P = (L + 1) >> 1;    // packed complex lines
+        cplx<T>* z = buf0;
+        cplx<T>* other = buf1;
+        if (MODE == 1) {
+            for (int idx = threadIdx.x; idx < P * n; idx += blockDim.x) {
+                const int p = idx / n, k = idx - p * n;
+                const bool hi = 2 * k > n;
+                const int kk = hi ? n - k : k;
+                const int la = 2 * p, lb = 2 * p + 1;
+                cplx<T> A = spec[(la % S) * cs + (long)(row0 + la / S) * nh + kk];
+                cplx<T> B = {T(0), T(0)};
+                if (lb < L) B = spec[(lb % S) * cs + (long)(row0 + lb / S) * nh + kk];
+                if (hi) {
+                    A = cconj(A);
+                    B = cconj(B);
+                }
+                z[idx] = {A.x - B.y, A.y + B.x};
+            }
+            __syncthreads();
+            z = fft_lines<T>(buf0, buf1, P, ax, +1);
+            other = (z == buf0) ? buf1 : buf0;
+            __syncthreads();
+        }
+        for (int idx = threadIdx.x; idx < rows * n; idx += blockDim.x) {
+            const int r = idx / n, y = idx - r * n;
+            const long v = (long)(row0 + r) * n + y;
+            double sn[S];
+#pragma unroll
+            for (int c = 0; c < S; ++c) {
+                const double so = a.eps_s[(long)c * N + v];
+                if (MODE == 1) {
+                    const int l = r * S + c;
+                    const cplx<T> zz = z[(l >> 1) * n + y];
+                    const double et = (double)((l & 1) ? zz.y : zz.x) * a.inv_n;
+                    sn[c] = a.ebar_s[c] + et;
+                    const double wc = c < D ? 1.0 : 2.0;
+                    const double d = sn[c] - so;
+                    part[0] += wc * d * d;
+                    part[1] += wc * so * so;
+                } else {
+                    sn[c] = a.warm ? so + shift[c] : a.ebar_s[c];
+                }
+                a.eps_s[(long)c * N + v] = sn[c];
+            }
+            const double lam = a.lam[v], mu = a.mu[v];
+            double e[S];
+#pragma unroll
+            for (int c = 0; c < S; ++c) e[c] = a.epsp_s ? sn[c] - a.epsp_s[(long)c * N + v] : sn[c];
+            double tr = 0.0, tr0 = 0.0;
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                tr += e[c];
+                tr0 += sn[c];
+            }
+#pragma unroll
+            for (int c = 0; c < S; ++c) {
+                const double sig = 2.0 * mu * e[c] + (c < D ? lam * tr : 0.0);
+                const double sig0 = 2.0 * a.mu0 * sn[c] + (c < D ? a.lam0 * tr0 : 0.0);
+                part[2 + c] += sn[c];
+                part[2 + S + c] += sig;
+                const int l = r * S + c;
+                cplx<T>* cell = &z[(l >> 1) * n + y];
+                if (l & 1) {
+                    cell->y = (T)(sig - sig0);
+                } else {
+                    cell->x = (T)(sig - sig0);
+                    if (l + 1 == L) cell->y = T(0);
+                }
+            }
+        }
+        __syncthreads();
+        cplx<T>* Z = fft_lines<T>(z, other, P, ax, -1);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < P * nh; idx += blockDim.x) {
+            const int p = idx / nh, k = idx - p * nh;
+            const cplx<T> zk = Z[p * n + k];
+            const cplx<T> zm = cconj(Z[p * n + (k == 0 ? 0 : n - k)]);
+            const int la = 2 * p, lb = 2 * p + 1;
+            const cplx<T> A = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y + zm.y)};
+            spec[(la % S) * cs + (long)(row0 + la / S) * nh + k] = A;
+            if (lb < L) {
+                const cplx<T> B = {T(0.5) * (zk.y - zm.y), T(-0.5) * (zk.x - zm.x)};
+                spec[(lb % S) * cs + (long)(row0 + lb / S) * nh + k] = B;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Strided pass along axis `axis` (not the contiguous one) over tiles of tk
+// adjacent half-spectrum columns.  KIND 0: forward only; 1: inverse only;
+// 2: forward, Green operator, inverse (the last non-contiguous axis, x).
+template <int D, typename T, int KIND>
+MGK_DEV void strided_pass(const LsArgs& a, int axis, cplx<T>* buf0, cplx<T>* buf1) {
+    constexpr int S = D == 2 ? 3 : 6;
+    const int nh = a.nh;
+    const int n = a.dims[axis];
+    cplx<T>* spec = reinterpret_cast<cplx<T>*>(a.spec);
+    const long cs = (long)a.nrows * nh;
+    long st, os;
+    int no;
+    if (D == 2) {
+        st = nh; no = 1; os = 0;
+    } else if (axis == 1) {
+        st = nh; no = a.dims[0]; os = (long)a.dims[1] * nh;
+    } else {
+        st = (long)a.dims[1] * nh; no = a.dims[1]; os = nh;
+    }
+    const int tk = a.tk;
+    const int ntk = (nh + tk - 1) / tk;
+    const int items = no * ntk;
+    const int nl = S * tk;
+    const FftAxis& fx = a.ax[axis];
+    for (int it = blockIdx.x; it < items; it += gridDim.x) {
+        const int o = it / ntk;
+        const int k0 = (it - o * ntk) * tk;
+        const int tku = min(tk, nh - k0);
+        const long base = o * os + k0;
+        for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+            const int t = idx % tk;
+            const int i = (idx / tk) % n;
+            const int c = idx / (tk * n);
+            buf0[(c * tk + t) * n + i] = (t < tku) ? spec[c * cs + base + t + i * st] : cplx<T>{T(0), T(0)};
+        }
+        __syncthreads();
+        cplx<T>* Z = fft_lines<T>(buf0, buf1, nl, fx, KIND == 1 ? +1 : -1);
+        __syncthreads();
+        if (KIND == 2) {
+            for (int idx = threadIdx.x; idx < tku * n; idx += blockDim.x) {
+                const int t = idx / n, kx = idx - t * n;
+                double q[3];
+                bool nyq[3];
+                q[0] = kfreq(kx, a.dims[0], a.pixel);
+                nyq[0] = (a.dims[0] % 2 == 0) && (2 * kx == a.dims[0]);
+                if (D == 2) {
+                    const int ky = k0 + t;
+                    q[1] = kfreq(ky, a.dims[1], a.pixel);
+                    nyq[1] = (a.dims[1] % 2 == 0) && (2 * ky == a.dims[1]);
+                } else {
+                    const int ky = o, kz = k0 + t;
+                    q[1] = kfreq(ky, a.dims[1], a.pixel);
+                    nyq[1] = (a.dims[1] % 2 == 0) && (2 * ky == a.dims[1]);
+                    q[2] = kfreq(kz, a.dims[2], a.pixel);
+                    nyq[2] = (a.dims[2] % 2 == 0) && (2 * kz == a.dims[2]);
+                }
+                cplx<T> tv[S];
+#pragma unroll
+                for (int c = 0; c < S; ++c) tv[c] = Z[(c * tk + t) * n + kx];
+                green_apply<D, T>(q, nyq, tv, a.inv2mu0, a.bcoef);
+#pragma unroll
+                for (int c = 0; c < S; ++c) Z[(c * tk + t) * n + kx] = tv[c];
+            }
+            __syncthreads();
+            cplx<T>* other = (Z == buf0) ? buf1 : buf0;
+            Z = fft_lines<T>(Z, other, nl, fx, +1);
+            __syncthreads();
+        }
+        for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
+            const int t = idx % tk;
+            const int i = (idx / tk) % n;
+            const int c = idx / (tk * n);
+            if (t < tku) spec[c * cs + base + t + i * st] = Z[(c * tk + t) * n + i];
+        }
+        __syncthreads();
+    }
+}
+
+template <int NP>
+MGK_DEV void publish_partials(const LsArgs& a, double* part, double* red) {
+    block_sum<NP>(part, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NP; ++k) a.partials[blockIdx.x * kMaxPartials + k] = part[k];
+}
+
+// Every CTA reduces all partials in the same fixed order -> identical values.
+template <int NP>
+MGK_DEV void gather_partials(const LsArgs& a, double* out /* shared, NP */) {
+    if (threadIdx.x < NP) {
+        double s = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(&a.partials[b * kMaxPartials + threadIdx.x]);
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+template <int D, typename T>
+__global__ void __launch_bounds__(256) ls_kernel(const __grid_constant__ LsArgs a) {
+    constexpr int S = D == 2 ? 3 : 6;
+    constexpr int NP = 2 + 2 * S;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[NP * 32];
+    __shared__ double vals[NP];
+    __shared__ double s_shift[6];
+    cplx<T>* buf0 = reinterpret_cast<cplx<T>*>(smem_raw);
+    cplx<T>* buf1 = reinterpret_cast<cplx<T>*>(smem_raw + a.smem_half);
+    const GridBar gb{a.bar, gridDim.x, a.err};
+    double shift[6] = {0, 0, 0, 0, 0, 0};
+    if (a.warm) {
+        double acc[NP];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) acc[k] = 0.0;
+        const int nchunks = (a.nrows + a.rpb - 1) / a.rpb;
+        for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+            const long v0 = (long)ch * a.rpb * a.nr;
+            const long v1 = min((long)a.N, v0 + (long)a.rpb * a.nr);
+            for (long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
+#pragma unroll
+                for (int c = 0; c < S; ++c) acc[c] += a.eps_s[(long)c * a.N + v];
+        }
+        publish_partials<NP>(a, acc, red);
+        if (!grid_sync(gb)) return;
+        gather_partials<NP>(a, vals);
+        if (threadIdx.x < S) s_shift[threadIdx.x] = a.ebar_s[threadIdx.x] - vals[threadIdx.x] * a.inv_n;
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < S; ++c) shift[c] = s_shift[c];
+        if (!grid_sync(gb)) return;
+    }
+    double part[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) part[k] = 0.0;
+    row_pass<D, T, 0>(a, buf0, buf1, part, shift);
+    publish_partials<NP>(a, part, red);
+    if (!grid_sync(gb)) return;
+    gather_partials<NP>(a, vals);
+    int it = 0;
+    double diff = 0.0;
+    while (it < a.max_iter) {
+        if (D == 3) {
+            strided_pass<D, T, 0>(a, 1, buf0, buf1);
+            if (!grid_sync(gb)) return;
+        }
+        strided_pass<D, T, 2>(a, 0, buf0, buf1);
+        if (!grid_sync(gb)) return;
+        if (D == 3) {
+            strided_pass<D, T, 1>(a, 1, buf0, buf1);
+            if (!grid_sync(gb)) return;
+        }
+#pragma unroll
+        for (int k = 0; k < NP; ++k) part[k] = 0.0;
+        row_pass<D, T, 1>(a, buf0, buf1, part, shift);
+        publish_partials<NP>(a, part, red);
+        if (!grid_sync(gb)) return;
+        gather_partials<NP>(a, vals);
+        const double dx = it == 0 ? a.diff_extra_first : 0.0;
+        const double nx = it == 0 ? a.norm_extra_first : a.norm_extra;
+        ++it;
+        diff = sqrt(vals[0] + dx) / (sqrt(vals[1] + nx) + 1e-20);
+        if (diff < a.tol) break;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.result->iters = it;
+        a.result->diff = diff;
+        for (int c = 0; c < S; ++c) {
+            a.result->sum_s[c] = vals[2 + c];
+            a.result->sum_sig[c] = vals[2 + S + c];
+        }
+    }
+}
+
+// full row-major DxD tensors from the symmetric storage (+ uniform antisymmetric part)
+template <int D>
+__global__ void full_tensor_kernel(const double* __restrict__ s, const double* __restrict__ epsp, const double* __restrict__ lam,
+                                   const double* __restrict__ mu, double w0, double w1, double w2, int N, int want_sig,
+                                   double* __restrict__ out) {
+    constexpr int S = D == 2 ? 3 : 6;
+    const double w[3] = {w0, w1, w2};
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < N; v += (long)gridDim.x * blockDim.x) {
+        double e[S], ep[S];
+#pragma unroll
+        for (int c = 0; c < S; ++c) {
+            e[c] = s[(long)c * N + v];
+            ep[c] = epsp ? epsp[(long)c * N + v] : 0.0;
+        }
+        double* o = out + v * D * D;
+        if (!want_sig) {
+#pragma unroll
+            for (int i = 0; i < D; ++i)
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    const double ww = (i == j) ? 0.0 : w[(D == 2) ? 0 : (i + j - 1)];
+                    o[i * D + j] = e[sym_idx(D, i, j)] + (i < j ? ww : -ww);
+                }
+        } else {
+            double tr = 0.0;
+#pragma unroll
+            for (int c = 0; c < D; ++c) tr += e[c] - ep[c];
+            const double m2 = 2.0 * mu[v], l = lam[v];
+#pragma unroll
+            for (int i = 0; i < D; ++i)
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    const int c = sym_idx(D, i, j);
+                    if (i == j) {
+                        o[i * D + j] = m2 * (e[c] - ep[c]) + l * tr;
+                    } else {
+                        const double ww = w[(D == 2) ? 0 : (i + j - 1)];
+                        o[i * D + j] = m2 * (e[c] + (i < j ? ww : -ww) - ep[c]);
+                    }
+                }
+        }
+    }
+}
+
+template <int D>
+__global__ void split_tensor_kernel(const double* __restrict__ full, int N, double* __restrict__ s) {
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < N; v += (long)gridDim.x * blockDim.x) {
+        const double* f = full + v * D * D;
+        for (int i = 0; i < D; ++i)
+            for (int j = i; j < D; ++j) s[(long)sym_idx(D, i, j) * N + v] = (i == j) ? f[i * D + i] : 0.5 * (f[i * D + j] + f[j * D + i]);
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned) {
+    std::memset(ax, 0, sizeof(*ax));
+    ax->n = n;
+    int m = n, k = 0;
+    while (m % 8 == 0 && m >= 64 && k < kMaxStages) { ax->radix[k++] = 8; m /= 8; }
+    while (m % 4 == 0 && k < kMaxStages) { ax->radix[k++] = 4; m /= 4; }
+    static const int primes[] = {2, 3, 5, 7, 11, 13};
+    for (int p : primes)
+        while (m % p == 0 && k < kMaxStages) { ax->radix[k++] = p; m /= p; }
+    if (m != 1) return false;
+    ax->nst = k;
+    std::vector<double> t64(2 * (size_t)n);
+    std::vector<float> t32(2 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)i / (long double)n;
+        t64[2 * i] = (double)cosl(ang);
+        t64[2 * i + 1] = (double)sinl(ang);
+        t32[2 * i] = (float)cosl(ang);
+        t32[2 * i + 1] = (float)sinl(ang);
+    }
+    void *d64 = nullptr, *d32 = nullptr;
+    if (cudaMalloc(&d64, sizeof(double) * 2 * n) != cudaSuccess) return false;
+    if (cudaMalloc(&d32, sizeof(float) * 2 * n) != cudaSuccess) return false;
+    cudaMemcpy(d64, t64.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d32, t32.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice);
+    owned->push_back(d64);
+    owned->push_back(d32);
+    ax->tw64 = reinterpret_cast<const cplx<double>*>(d64);
+    ax->tw32 = reinterpret_cast<const cplx<float>*>(d32);
+    return true;
+}
+
+static void lame(double E, double nu, int D, bool ps, double* lam, double* mu) {
+    // compute_lame_2d / compute_lame_3d (linear_elastic_solver.hpp:36-45, :315-319)
+    *mu = E / (2.0 * (1.0 + nu));
+    if (D == 2 && ps) *lam = E * nu / (1.0 - nu * nu);
+    else *lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+}
+
+#define MGK_CK(x)                                                        \
+    do {                                                                 \
+        cudaError_t e_ = (x);                                            \
+        if (e_ != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e_)); \
+    } while (0)
+
+LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, const double* E, const double* nu, cudaStream_t stream)
+    : D_(D), S_(n_sym(D)), plane_stress_(plane_stress), pixel_(pixel), stream_(stream) {
+    if (D != 2 && D != 3) throw std::invalid_argument("dimension must be 2 or 3");
+    dims_[0] = dims[0];
+    dims_[1] = dims[1];
+    dims_[2] = D == 3 ? dims[2] : 1;
+    for (int i = 0; i < D; ++i)
+        if (dims_[i] < 1) throw std::invalid_argument("grid sizes must be positive");
+    long N = (long)dims_[0] * dims_[1] * dims_[2];
+    if (N > (1L << 30)) throw std::invalid_argument("grid too large");
+    N_ = (int)N;
+    // reference medium from voxel means (serial sums as linear_elastic_solver.hpp:164-169)
+    double Es = 0.0, ns = 0.0;
+    for (long i = 0; i < N; ++i) {
+        Es += E[i];
+        ns += nu[i];
+    }
+    lame(Es / N, ns / N, D, plane_stress, &lam0_, &mu0_);
+    std::vector<double> lam(N), mu(N);
+    sum_two_mu_ = 0.0;
+    for (long i = 0; i < N; ++i) {
+        lame(E[i], nu[i], D, plane_stress, &lam[i], &mu[i]);
+        sum_two_mu_ += 2.0 * mu[i];
+    }
+    const int nr = dims_[D - 1];
+    const int nh = nr / 2 + 1;
+    const int nrows = (int)(N / nr);
+    LsArgs& a = args_;
+    a.D = D;
+    a.S = S_;
+    for (int i = 0; i < 3; ++i) a.dims[i] = dims_[i];
+    a.N = N_;
+    a.nr = nr;
+    a.nh = nh;
+    a.nrows = nrows;
+    a.inv_n = 1.0 / (double)N;
+    a.lam0 = lam0_;
+    a.mu0 = mu0_;
+    a.inv2mu0 = 1.0 / (2.0 * mu0_);
+    a.bcoef = (lam0_ + mu0_) / (mu0_ * (lam0_ + 2.0 * mu0_));
+    a.pixel = pixel;
+    for (int i = 0; i < D; ++i)
+        if (!plan_axis(dims_[i], &a.ax[i], &tw_bufs_)) throw std::invalid_argument("unsupported FFT length (prime factor > 13)");
+    // decomposition
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    a.rpb = (S_ == 3) ? 2 : 1;
+    if ((long)nrows / a.rpb < nsm / 2 && a.rpb > 1) a.rpb = 1;
+    int no = (D == 2) ? 1 : std::max(dims_[0], dims_[1]);
+    a.tk = ((long)no * nh >= 4L * nsm) ? 2 : 1;
+    const int row_items = (nrows + a.rpb - 1) / a.rpb;
+    const int col_items = ((D == 2) ? 1 : std::min(dims_[0], dims_[1])) * ((nh + a.tk - 1) / a.tk);
+    // shared memory: two buffers of the largest pass
+    const size_t elem = sizeof(cplx<double>);
+    const size_t row_b = (size_t)((a.rpb * S_ + 1) / 2) * nr * elem;
+    size_t col_b = 0;
+    for (int ax = 0; ax < D - 1; ++ax) col_b = std::max(col_b, (size_t)S_ * a.tk * dims_[ax] * elem);
+    const size_t half_b = (std::max(row_b, col_b) + 127) / 128 * 128;
+    smem_ = 2 * half_b;
+    a.smem_half = (int)half_b;
+    if (smem_ > 200 * 1024) throw std::invalid_argument("grid axis too long for the shared-memory FFT");
+    auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
+    MGK_CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
+    int per_sm = 0;
+    MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads_, smem_));
+    if (per_sm < 1) throw std::runtime_error("LS kernel does not fit on an SM");
+    grid_ = std::min(std::max(row_items, col_items), per_sm * nsm);
+    grid_ = std::max(grid_, 1);
+    // buffers
+    bytes_ = 0;
+    auto alloc = [&](void** p, size_t b) {
+        MGK_CK(cudaMalloc(p, b));
+        bytes_ += b;
+    };
+    alloc((void**)&d_eps_s_, sizeof(double) * S_ * N);
+    alloc((void**)&d_lam_, sizeof(double) * N);
+    alloc((void**)&d_mu_, sizeof(double) * N);
+    alloc(&d_spec_, elem * S_ * (size_t)nrows * nh);
+    alloc((void**)&d_partials_, sizeof(double) * kMaxPartials * grid_);
+    alloc((void**)&d_res_, sizeof(LsResult));
+    alloc((void**)&d_bar_, sizeof(unsigned) * 4);
+    MGK_CK(cudaMemcpy(d_lam_, lam.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+    MGK_CK(cudaMemcpy(d_mu_, mu.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+    MGK_CK(cudaMemset(d_eps_s_, 0, sizeof(double) * S_ * N));
+    MGK_CK(cudaMemset(d_bar_, 0, sizeof(unsigned) * 4));
+    MGK_CK(cudaMemset(d_res_, 0, sizeof(LsResult)));
+    a.eps_s = d_eps_s_;
+    a.lam = d_lam_;
+    a.mu = d_mu_;
+    a.spec = d_spec_;
+    a.partials = d_partials_;
+    a.result = d_res_;
+    a.bar = d_bar_;
+    a.err = d_bar_ + 2;
+}
+
+LsSolver::~LsSolver() {
+    cudaFree(d_eps_s_);
+    cudaFree(d_lam_);
+    cudaFree(d_mu_);
+    cudaFree(d_spec_);
+    cudaFree(d_partials_);
+    cudaFree(d_res_);
+    cudaFree(d_bar_);
+    for (void* p : tw_bufs_) cudaFree(p);
+}
+
+cudaError_t LsSolver::solve(const double* ebar, bool warm, const double* epsp_s, int max_iter, double tol) {
+    LsArgs a = args_;
+    const int D = D_;
+    double wbar[3] = {0, 0, 0};
+    for (int i = 0; i < D; ++i)
+        for (int j = i; j < D; ++j) {
+            const int c = sym_idx(D, i, j);
+            a.ebar_s[c] = (i == j) ? ebar[i * D + i] : 0.5 * (ebar[i * D + j] + ebar[j * D + i]);
+            if (i != j) wbar[(D == 2) ? 0 : (i + j - 1)] = 0.5 * (ebar[i * D + j] - ebar[j * D + i]);
+        }
+    const int noff = D == 2 ? 1 : 3;
+    double sw2 = 0.0, sdev = 0.0;
+    for (int k = 0; k < noff; ++k) {
+        sw2 += wbar[k] * wbar[k];
+        sdev += asym_dev2_[k];
+    }
+    a.norm_extra = 2.0 * (double)N_ * sw2;
+    if (warm) {
+        a.norm_extra_first = 2.0 * (sdev + (double)N_ * sw2);
+        a.diff_extra_first = 2.0 * sdev;
+    } else {
+        a.norm_extra_first = a.norm_extra;
+        a.diff_extra_first = 0.0;
+    }
+    for (int k = 0; k < 3; ++k) {
+        w_[k] = wbar[k];
+        asym_dev2_[k] = 0.0;
+    }
+    a.warm = warm ? 1 : 0;
+    a.max_iter = max_iter;
+    a.tol = tol;
+    a.epsp_s = epsp_s;
+    void* params[] = {&a};
+    auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
+    cudaError_t e = cudaLaunchCooperativeKernel(kfn, dim3(grid_), dim3(threads_), params, smem_, stream_);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(&h_res_, d_res_, sizeof(LsResult), cudaMemcpyDeviceToHost, stream_);
+}
+
+void LsSolver::macro(double* em, double* sm, int* iters) const {
+    const int D = D_;
+    const double invN = 1.0 / (double)N_;
+    const double mean2mu = sum_two_mu_ * invN;
+    for (int i = 0; i < D; ++i)
+        for (int j = 0; j < D; ++j) {
+            const int c = sym_idx(D, i, j);
+            const double w = (i == j) ? 0.0 : w_[(D == 2) ? 0 : (i + j - 1)];
+            const double sgn = (i < j) ? 1.0 : -1.0;
+            em[i * D + j] = h_res_.sum_s[c] * invN + sgn * w;
+            sm[i * D + j] = h_res_.sum_sig[c] * invN + sgn * w * mean2mu;
+        }
+    if (iters) *iters = h_res_.iters;
+}
+
+unsigned LsSolver::device_error() const {
+    unsigned e = 0;
+    cudaMemcpy(&e, d_bar_ + 2, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    return e;
+}
+
+void LsSolver::clear_error() { cudaMemset(d_bar_, 0, sizeof(unsigned) * 4); }
+
+cudaError_t LsSolver::download_eps(double* host) const {
+    double* tmp = nullptr;
+    size_t b = sizeof(double) * (size_t)N_ * D_ * D_;
+    cudaError_t e = cudaMalloc(&tmp, b);
+    if (e != cudaSuccess) return e;
+    if (D_ == 2) full_tensor_kernel<2><<<256, 256, 0, stream_>>>(d_eps_s_, nullptr, d_lam_, d_mu_, w_[0], w_[1], w_[2], N_, 0, tmp);
+    else full_tensor_kernel<3><<<256, 256, 0, stream_>>>(d_eps_s_, nullptr, d_lam_, d_mu_, w_[0], w_[1], w_[2], N_, 0, tmp);
+    e = cudaMemcpyAsync(host, tmp, b, cudaMemcpyDeviceToHost, stream_);
+    cudaStreamSynchronize(stream_);
+    cudaFree(tmp);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t LsSolver::download_sig(const double* epsp_s, double* host) const {
+    double* tmp = nullptr;
+    size_t b = sizeof(double) * (size_t)N_ * D_ * D_;
+    cudaError_t e = cudaMalloc(&tmp, b);
+    if (e != cudaSuccess) return e;
+    if (D_ == 2) full_tensor_kernel<2><<<256, 256, 0, stream_>>>(d_eps_s_, epsp_s, d_lam_, d_mu_, w_[0], w_[1], w_[2], N_, 1, tmp);
+    else full_tensor_kernel<3><<<256, 256, 0, stream_>>>(d_eps_s_, epsp_s, d_lam_, d_mu_, w_[0], w_[1], w_[2], N_, 1, tmp);
+    e = cudaMemcpyAsync(host, tmp, b, cudaMemcpyDeviceToHost, stream_);
+    cudaStreamSynchronize(stream_);
+    cudaFree(tmp);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t LsSolver::upload_eps(const double* host) {
+    const int D = D_;
+    // antisymmetric part: mean and spread per off-diagonal pair
+    double mean[3] = {0, 0, 0}, dev[3] = {0, 0, 0};
+    const int noff = D == 2 ? 1 : 3;
+    const int pi[3] = {0, 0, 1}, pj[3] = {1, 2, 2};
+    for (int k = 0; k < noff; ++k) {
+        const int i = pi[k], j = pj[k];
+        double s = 0.0;
+        for (int v = 0; v < N_; ++v) s += 0.5 * (host[(size_t)v * D * D + i * D + j] - host[(size_t)v * D * D + j * D + i]);
+        mean[k] = s / N_;
+        double d2 = 0.0;
+        for (int v = 0; v < N_; ++v) {
+            const double a = 0.5 * (host[(size_t)v * D * D + i * D + j] - host[(size_t)v * D * D + j * D + i]) - mean[k];
+            d2 += a * a;
+        }
+        dev[k] = d2;
+    }
+    for (int k = 0; k < 3; ++k) {
+        w_[k] = mean[k];
+        asym_dev2_[k] = dev[k];
+    }
+    double* tmp = nullptr;
+    size_t b = sizeof(double) * (size_t)N_ * D * D;
+    cudaError_t e = cudaMalloc(&tmp, b);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(tmp, host, b, cudaMemcpyHostToDevice, stream_);
+    if (D == 2) split_tensor_kernel<2><<<256, 256, 0, stream_>>>(tmp, N_, d_eps_s_);
+    else split_tensor_kernel<3><<<256, 256, 0, stream_>>>(tmp, N_, d_eps_s_);
+    cudaStreamSynchronize(stream_);
+    cudaFree(tmp);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+}  // namespace mgk

@@ -1,0 +1,128 @@
+// Lippmann-Schwinger (Moulinec-Suquet basic scheme) solver on the GPU.
+//
+// Replaces spectral_solver_2d / spectral_solver_3d of linear_elastic_solver.hpp
+// (:146-309, :431-593) and the stored Green tensor of green_operator_2d/3d
+// (:70-119, :344-396).  Design (B200):
+//  * state in HBM, structure-of-arrays FP64: the symmetric part of the strain
+//    (3 components in 2D, 6 in 3D) plus, per solve, the constant antisymmetric
+//    part of the macroscopic strain (the reference keeps full 2x2 / 3x3
+//    tensors; their antisymmetric part is always uniform, see ls.cu);
+//  * one persistent cooperative kernel per solve: all iterations, the
+//    convergence test and the macro averages run on the device, separated by
+//    bounded grid barriers; no host round trip per iteration;
+//  * real-to-complex transforms along the contiguous axis by packing two real
+//    component lines into one complex FFT; strided passes along the other axes
+//    on tiles staged through shared memory; the Green operator is applied in
+//    closed form per k-point inside the last strided pass (no 16/81-double
+//    tensor per voxel is stored or streamed).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "fft.cuh"
+
+namespace mgk {
+
+constexpr int kMaxPartials = 16;
+
+struct LsResult {
+    int iters;
+    int pad;
+    double diff;
+    double sum_s[6];
+    double sum_sig[6];
+};
+
+struct LsArgs {
+    int D, S;
+    int dims[3];
+    int N, nr, nh, nrows;  // voxels, contiguous-axis length, its half spectrum, rows = N / nr
+    int rpb;               // rows per row-pass chunk
+    int tk;                // columns per strided-pass tile
+    int max_iter;
+    int warm;
+    double tol;
+    double inv_n;          // 1 / N
+    double norm_extra;     // 2 N sum_offdiag w^2: antisymmetric part of |eps|^2 (uniform field)
+    double norm_extra_first;  // same for the first iteration (warm start of a non-uniform field)
+    double diff_extra_first;  // antisymmetric part of |eps_new - eps|^2 in the first iteration
+    int smem_half;         // byte offset of the second shared-memory buffer
+    double ebar_s[6];      // symmetric part of the prescribed mean strain
+    double lam0, mu0, inv2mu0, bcoef;
+    double pixel;
+    // device arrays
+    double* eps_s;         // S x N
+    const double* epsp_s;  // S x N or null
+    const double* lam;     // N
+    const double* mu;      // N
+    void* spec;            // S x nrows x nh complex (T)
+    double* partials;      // gridDim.x x kMaxPartials
+    LsResult* result;
+    unsigned* bar;
+    unsigned* err;
+    FftAxis ax[3];         // per axis (x, y, z)
+};
+
+class LsSolver {
+public:
+    // dims: {nx, ny} (D=2) or {nx, ny, nz}; E, nu host arrays of N values.
+    LsSolver(int D, const int* dims, bool plane_stress, double pixel, const double* E, const double* nu, cudaStream_t stream);
+    ~LsSolver();
+    LsSolver(const LsSolver&) = delete;
+    LsSolver& operator=(const LsSolver&) = delete;
+
+    // Enqueue one solve on the stream.  ebar: full DxD row-major.  warm: keep the
+    // current field and shift its mean to ebar (else fill with ebar).  epsp_s:
+    // device S x N plastic strain or null.  Returns a cudaError_t.
+    cudaError_t solve(const double* ebar, bool warm, const double* epsp_s, int max_iter, double tol);
+
+    // After the stream has synchronised: mean strain / stress (full DxD
+    // row-major) of the last solve and its iteration count.
+    void macro(double* eps_macro, double* sig_macro, int* iters) const;
+    const LsResult& host_result() const { return h_res_; }
+    LsResult* device_result() const { return d_res_; }
+    unsigned device_error() const;  // syncs
+    void clear_error();
+
+    // Full-tensor fields (row-major DxD per voxel) to host; syncs.
+    cudaError_t download_eps(double* host) const;
+    cudaError_t download_sig(const double* epsp_s, double* host) const;
+    cudaError_t upload_eps(const double* host);  // full tensors; sets the antisymmetric part
+
+    int D() const { return D_; }
+    int S() const { return S_; }
+    int N() const { return N_; }
+    double* eps_s() { return d_eps_s_; }
+    const double* lam() const { return d_lam_; }
+    const double* mu() const { return d_mu_; }
+    double asym(int k) const { return w_[k]; }
+    cudaStream_t stream() const { return stream_; }
+    int grid() const { return grid_; }
+    size_t device_bytes() const { return bytes_; }
+
+private:
+    int D_, S_, N_;
+    int dims_[3];
+    bool plane_stress_;
+    double pixel_;
+    double lam0_, mu0_, sum_two_mu_;
+    double w_[3] = {0, 0, 0};  // antisymmetric half-differences (xy, xz, yz): mean over voxels
+    double asym_dev2_[3] = {0, 0, 0};  // sum over voxels of (a_v - w)^2 (non-uniform uploads)
+    cudaStream_t stream_;
+    double *d_eps_s_ = nullptr, *d_lam_ = nullptr, *d_mu_ = nullptr, *d_partials_ = nullptr;
+    void* d_spec_ = nullptr;
+    LsResult* d_res_ = nullptr;
+    LsResult h_res_{};
+    unsigned* d_bar_ = nullptr;  // {arrivals, generation, err}
+    std::vector<void*> tw_bufs_;
+    LsArgs args_{};
+    int grid_ = 1, threads_ = 256;
+    size_t smem_ = 0, bytes_ = 0;
+};
+
+// Plans the radix sequence of a length-n transform (radix-4 first, then 2, 3,
+// 5, 7, 8, 11, 13).  Returns false for lengths with other prime factors.
+bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned);
+
+}  // namespace mgk
