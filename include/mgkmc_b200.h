@@ -118,9 +118,19 @@ MGK_API mgk_status mgk_kmc_elastic_run(mgk_kmc* h);
  * 10 nu_field (N).  Returns the element count in *count when dst is NULL. */
 MGK_API mgk_status mgk_kmc_get_field(mgk_kmc* h, int field, double* dst, long long* count);
 /* eps_macro (D*D), sig_macro (D*D), time, then counters: thermal events,
- * cascades, LS solves, LS iterations, elastic steps, selection margin min. */
+ * cascades, LS solves, LS iterations, elastic steps, selection margin min,
+ * host synchronisations, kernel launches. */
 MGK_API mgk_status mgk_kmc_get_macro(mgk_kmc* h, double* out, int n);
 MGK_API void mgk_kmc_destroy(mgk_kmc* h);
+
+/* Measurement hooks (no counterpart in the reference, which only logs wall
+ * time).  mgk_kmc_set_profiling(h, 1) clears the profile and records CUDA
+ * events around every LS solve, sweep and selection on the engine's stream.
+ * mgk_kmc_get_profile fills out[0..9] = {ls_ms, ls_launches, ls_iterations,
+ * sweep_ms, sweeps, select_ms, selects, run_ms, events_timed, 0} and copies up
+ * to lat_cap per-event host latencies (microseconds) into lat. */
+MGK_API mgk_status mgk_kmc_set_profiling(mgk_kmc* h, int on);
+MGK_API mgk_status mgk_kmc_get_profile(mgk_kmc* h, double* out, double* lat, long long lat_cap);
 
 #ifdef __cplusplus
 }

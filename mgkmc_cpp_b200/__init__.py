@@ -221,7 +221,7 @@ class _KmcBase:
         raise AttributeError(name)
 
     def macro(self) -> np.ndarray:
-        out = np.zeros(2 * self.D * self.D + 9)
+        out = np.zeros(2 * self.D * self.D + 10)
         _lib.check(_lib.lib().mgk_kmc_get_macro(self._h, _lib.dptr(out), out.size))
         return out
 
@@ -241,8 +241,21 @@ class _KmcBase:
     @property
     def stats(self) -> dict:
         m = self.macro()[2 * self.D * self.D + 1:]
-        keys = ["thermal_events", "cascades", "ls_solves", "ls_iters", "elastic_steps", "min_margin", "syncs"]
+        keys = ["thermal_events", "cascades", "ls_solves", "ls_iters", "elastic_steps", "min_margin", "syncs", "launches"]
         return {k: float(v) for k, v in zip(keys, m)}
+
+    def set_profiling(self, on: bool = True):
+        _lib.check(_lib.lib().mgk_kmc_set_profiling(self._h, int(bool(on))))
+
+    def profile(self, max_latencies: int = 1 << 20) -> dict:
+        out = np.zeros(10)
+        lat = np.zeros(max_latencies)
+        _lib.check(_lib.lib().mgk_kmc_get_profile(self._h, _lib.dptr(out), _lib.dptr(lat), max_latencies))
+        keys = ["ls_ms", "ls_launches", "ls_iterations", "sweep_ms", "sweeps", "select_ms", "selects", "run_ms",
+                "events_timed"]
+        d = {k: float(v) for k, v in zip(keys, out)}
+        d["event_us"] = lat[:int(min(out[8], max_latencies))].copy()
+        return d
 
     def close(self):
         if getattr(self, "_h", None):

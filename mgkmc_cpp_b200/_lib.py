@@ -16,7 +16,7 @@ STATUS = {0: "MGK_OK", 1: "MGK_LS_NOT_CONVERGED", 2: "MGK_BAD_SHAPE", 3: "MGK_OO
 
 EXPORTS = ["mgk_last_error", "mgk_version", "mgk_device_count", "mgk_ls_create", "mgk_ls_solve", "mgk_ls_destroy",
            "mgk_kmc_create", "mgk_kmc_run", "mgk_kmc_elastic_run", "mgk_kmc_get_field", "mgk_kmc_get_macro",
-           "mgk_kmc_destroy"]
+           "mgk_kmc_destroy", "mgk_kmc_set_profiling", "mgk_kmc_get_profile"]
 
 
 class MgkError(RuntimeError):
@@ -74,10 +74,12 @@ def lib():
     L.mgk_kmc_elastic_run.argtypes = [vp]
     L.mgk_kmc_get_field.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_longlong)]
     L.mgk_kmc_get_macro.argtypes = [vp, dp, C.c_int]
+    L.mgk_kmc_set_profiling.argtypes = [vp, C.c_int]
+    L.mgk_kmc_get_profile.argtypes = [vp, dp, dp, C.c_longlong]
     L.mgk_kmc_destroy.argtypes = [vp]
     L.mgk_kmc_destroy.restype = None
     for fn in ("mgk_ls_create", "mgk_ls_solve", "mgk_kmc_create", "mgk_kmc_run", "mgk_kmc_elastic_run",
-               "mgk_kmc_get_field", "mgk_kmc_get_macro"):
+               "mgk_kmc_get_field", "mgk_kmc_get_macro", "mgk_kmc_set_profiling", "mgk_kmc_get_profile"):
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L

@@ -188,6 +188,23 @@ mgk_status mgk_kmc_get_macro(mgk_kmc* h, double* out, int n) {
     return MGK_OK;
 }
 
+mgk_status mgk_kmc_set_profiling(mgk_kmc* h, int on) {
+    if (!h) return fail(MGK_BAD_ARG, "null argument");
+    h->eng->set_profiling(on != 0);
+    return MGK_OK;
+}
+
+mgk_status mgk_kmc_get_profile(mgk_kmc* h, double* out, double* lat, long long lat_cap) {
+    if (!h || !out) return fail(MGK_BAD_ARG, "null argument");
+    const mgk::EngineProfile& p = h->eng->profile();
+    double v[10] = {p.ls_ms, (double)p.ls_n, (double)p.ls_iters, p.sweep_ms, (double)p.sweep_n, p.select_ms,
+                    (double)p.select_n, p.run_ms, (double)p.event_us.size(), 0.0};
+    std::memcpy(out, v, sizeof(v));
+    if (lat)
+        for (long long i = 0; i < lat_cap && i < (long long)p.event_us.size(); ++i) lat[i] = p.event_us[i];
+    return MGK_OK;
+}
+
 void mgk_kmc_destroy(mgk_kmc* h) {
     if (!h) return;
     delete h->eng;

@@ -161,6 +161,8 @@ KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu)
     CK(cudaMemset(d_status_, 0, sizeof(KmcStatus)));
     CK(cudaMallocHost((void**)&h_status_, sizeof(KmcStatus)));
     CK(cudaMallocHost((void**)&h_lsres_, sizeof(LsResult)));
+    CK(cudaMallocHost((void**)&h_lserr_, sizeof(unsigned)));
+    *h_lserr_ = 0;
     std::memset(h_status_, 0, sizeof(KmcStatus));
     upload_cap_ = 1 + (size_t)M_ * (C_ + 1);
     alloc((void**)&d_upload_, sizeof(double) * upload_cap_);
@@ -196,6 +198,9 @@ KmcEngine::~KmcEngine() {
     cudaFreeHost(h_status_);
     cudaFreeHost(h_upload_);
     cudaFreeHost(h_lsres_);
+    cudaFreeHost(h_lserr_);
+    for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
     ls_.reset();
     if (st_) cudaStreamDestroy(st_);
 }
@@ -266,9 +271,51 @@ void KmcEngine::gen_flip_draws(double* out) {
     }
 }
 
+void KmcEngine::set_profiling(bool on) {
+    if (on && !ev_[0])
+        for (auto& e : ev_) cudaEventCreate(&e);
+    profiling_ = on;
+    prof_ = EngineProfile();
+}
+
+// event pairs: 0 LS solve, 1 sweep, 2 select+flip, 3 whole run
+void KmcEngine::prof_begin(int pair) {
+    if (profiling_) cudaEventRecord(ev_[2 * pair], st_);
+}
+void KmcEngine::prof_end(int pair) {
+    if (!profiling_) return;
+    cudaEventRecord(ev_[2 * pair + 1], st_);
+    if (pair == 0) ls_ev_pending_ = true;
+    if (pair == 1) sw_ev_pending_ = true;
+    if (pair == 2) sel_ev_pending_ = true;
+}
+// after a stream sync: fold the recorded intervals into the profile
+void KmcEngine::prof_collect() {
+    if (!profiling_) return;
+    float ms = 0.f;
+    if (ls_ev_pending_ && cudaEventElapsedTime(&ms, ev_[0], ev_[1]) == cudaSuccess) {
+        prof_.ls_ms += ms;
+        prof_.ls_n++;
+        prof_.ls_iters += h_lsres_->iters;
+    }
+    if (sw_ev_pending_ && cudaEventElapsedTime(&ms, ev_[2], ev_[3]) == cudaSuccess) {
+        prof_.sweep_ms += ms;
+        prof_.sweep_n++;
+    }
+    if (sel_ev_pending_ && cudaEventElapsedTime(&ms, ev_[4], ev_[5]) == cudaSuccess) {
+        prof_.select_ms += ms;
+        prof_.select_n++;
+    }
+    ls_ev_pending_ = sw_ev_pending_ = sel_ev_pending_ = false;
+}
+
 cudaError_t KmcEngine::enqueue_elastic() {
+    prof_begin(0);
+    stats_.launches += 1;
     cudaError_t e = ls_->solve(eps_macro_, true, dev_.epsp_s, p_.ls_max_iter, p_.ls_tol);
+    prof_end(0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_lsres_, ls_->device_result(), sizeof(LsResult), cudaMemcpyDeviceToHost, st_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_lserr_, ls_->device_error_ptr(), sizeof(unsigned), cudaMemcpyDeviceToHost, st_);
     ls_pending_ = true;
     return e;
 }
@@ -288,7 +335,10 @@ mgk_status KmcEngine::finish_elastic() {
 }
 
 cudaError_t KmcEngine::enqueue_sweep() {
+    prof_begin(1);
+    stats_.launches += 1;
     cudaError_t e = kmc_sweep(dev_, phys_, time_, d_blk_, d_blk_unst_, d_blk_last_, nblk_, items_, d_status_, st_);
+    prof_end(1);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_status_, d_status_, sizeof(KmcStatus), cudaMemcpyDeviceToHost, st_);
     return e;
 }
@@ -304,8 +354,11 @@ mgk_status KmcEngine::sync_status() {
         last_error = "device selection error";
         return MGK_CUDA_ERROR;
     }
-    unsigned le = 0;
-    (void)le;
+    if (ls_pending_ && *h_lserr_) {
+        last_error = "device wait timed out in the LS solver";
+        return MGK_DEVICE_TIMEOUT;
+    }
+    prof_collect();
     return finish_elastic();
 }
 
@@ -320,7 +373,8 @@ mgk_status KmcEngine::elastic_run() {
         last_error = cudaGetErrorString(e);
         return MGK_CUDA_ERROR;
     }
-    if (ls_->device_error()) {
+    prof_collect();
+    if (*h_lserr_) {
         last_error = "device wait timed out in the LS solver";
         return MGK_DEVICE_TIMEOUT;
     }
@@ -338,6 +392,7 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips) {
         int zero = 0;
         CK(cudaMemcpyAsync(&d_status_->n_collect, &zero, sizeof(int), cudaMemcpyHostToDevice, st_));
         CK(kmc_cascade_collect(dev_, phys_, d_ckeys_, d_cmodes_, d_status_, st_));
+        stats_.launches += 1;
         CK(cudaMemcpyAsync(&h_status_->n_collect, &d_status_->n_collect, sizeof(int), cudaMemcpyDeviceToHost, st_));
         CK(cudaStreamSynchronize(st_));
         stats_.syncs++;
@@ -357,6 +412,12 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips) {
         CK(cudaMemcpyAsync(d_upload_, h_upload_, sizeof(double) * need, cudaMemcpyHostToDevice, st_));
         CK(kmc_cascade_flip(dev_, phys_, d_ckeys_, d_cmodes_, n, d_ckeys2_, d_cmodes2_, time_, d_upload_,
                             p_.redraw_directions, p_.redraw_barriers, d_status_, st_));
+        {
+            int np2 = 1, lg = 0;
+            while (np2 < n) np2 <<= 1;
+            while ((1 << lg) < np2) ++lg;
+            stats_.launches += 1 + (np2 <= 8192 ? 1 : 1 + lg * (lg + 1) / 2);
+        }
         CK(enqueue_elastic());
         total += n;
         ++local;
@@ -507,9 +568,11 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
         f_summary_ = f_global_ = nullptr;
     };
     int elastic_done = 0, total_kmc = 0, step = 1, seq_instab = 0;
+    const long long events_at_start = stats_.thermal_events;
     const int max_seq = (int)(rp.max_kmc_steps_pct * (double)N_);
     mgk_status s;
     try {
+        if (profiling_) cudaEventRecord(ev_[6], st_);
         CK(enqueue_elastic());
         CK(enqueue_sweep());
         s = sync_status();
@@ -544,6 +607,7 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                     continue;
                 }
                 const double R = h_status_->total_hi + h_status_->total_lo;
+                const double t_ev = wall_seconds();
                 if (R > 0.0) {
                     const double u1 = U(rng_);
                     const double tw = -std::log(u1) / R;
@@ -555,8 +619,11 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                         gen_flip_draws(h_upload_ + 1);
                         const size_t nup = 1 + (size_t)((p_.redraw_directions || p_.redraw_barriers) ? M_ : 1) * (C_ + 1);
                         CK(cudaMemcpyAsync(d_upload_, h_upload_, sizeof(double) * nup, cudaMemcpyHostToDevice, st_));
+                        prof_begin(2);
+                        stats_.launches += 1;
                         CK(kmc_select_flip(dev_, phys_, d_blk_, d_blk_last_, nblk_, items_, d_upload_, time_, d_upload_ + 1,
                                            p_.redraw_directions, p_.redraw_barriers, d_status_, st_));
+                        prof_end(2);
                         CK(enqueue_elastic());
                         CK(enqueue_sweep());
                         s = sync_status();
@@ -565,6 +632,7 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                             return s;
                         }
                         stats_.thermal_events++;
+                        if (profiling_) prof_.event_us.push_back((wall_seconds() - t_ev) * 1e6);
                         if (h_status_->margin < stats_.min_margin) stats_.min_margin = h_status_->margin;
                         const bool instab = h_status_->is_instab != 0;
                         seq_instab = instab ? seq_instab + 1 : 0;
@@ -581,7 +649,7 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                         push(0, h_status_->selected, instab ? 1 : 0, R, tw);
                         total_kmc++;
                         step++;
-                        if (rp.max_events > 0 && stats_.thermal_events >= rp.max_events) {
+                        if (rp.max_events > 0 && stats_.thermal_events - events_at_start >= rp.max_events) {
                             stop = true;
                             break;
                         }
@@ -664,6 +732,12 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
         last_error = ex.what();
         close_logs();
         return MGK_CUDA_ERROR;
+    }
+    if (profiling_) {
+        float ms = 0.f;
+        cudaEventRecord(ev_[7], st_);
+        cudaEventSynchronize(ev_[7]);
+        if (cudaEventElapsedTime(&ms, ev_[6], ev_[7]) == cudaSuccess) prof_.run_ms += ms;
     }
     close_logs();
     if (rows_out) *rows_out = rows;
@@ -760,6 +834,7 @@ void KmcEngine::get_macro(double* out, int n) const {
     v.push_back((double)stats_.elastic_steps);
     v.push_back(stats_.min_margin);
     v.push_back((double)stats_.syncs);
+    v.push_back((double)stats_.launches);
     for (int i = 0; i < n && i < (int)v.size(); ++i) out[i] = v[i];
 }
 

@@ -27,8 +27,16 @@ struct BarrierGen {
 
 struct EngineStats {
     long long thermal_events = 0, cascades = 0, cascade_flips = 0, ls_solves = 0, ls_iters = 0, elastic_steps = 0;
-    long long syncs = 0;
+    long long syncs = 0, launches = 0;
     double min_margin = 1.0;
+};
+
+// Optional per-kernel timing with CUDA events on the engine's stream
+// (profiling mode): LS solves, sweeps, select+flip, plus per-event latency.
+struct EngineProfile {
+    double ls_ms = 0, sweep_ms = 0, select_ms = 0, run_ms = 0;
+    long long ls_n = 0, ls_iters = 0, sweep_n = 0, select_n = 0;
+    std::vector<double> event_us;  // host wall time per thermal event
 };
 
 class KmcEngine {
@@ -42,6 +50,8 @@ public:
     void get_macro(double* out, int n) const;
 
     const EngineStats& stats() const { return stats_; }
+    void set_profiling(bool on);
+    const EngineProfile& profile() const { return prof_; }
     int D() const { return D_; }
     std::string last_error;
 
@@ -85,6 +95,15 @@ private:
     LsResult* h_lsres_ = nullptr;    // pinned copy of the last LS result
     bool ls_pending_ = false;
     EngineStats stats_;
+    // profiling
+    bool profiling_ = false;
+    EngineProfile prof_;
+    cudaEvent_t ev_[8] = {};
+    void prof_begin(int pair);
+    void prof_end(int pair);
+    void prof_collect();
+    bool ls_ev_pending_ = false, sw_ev_pending_ = false, sel_ev_pending_ = false;
+    unsigned* h_lserr_ = nullptr;  // pinned copy of the LS error word
     // logging
     FILE* f_summary_ = nullptr;
     FILE* f_global_ = nullptr;

@@ -83,6 +83,7 @@ public:
     const LsResult& host_result() const { return h_res_; }
     LsResult* device_result() const { return d_res_; }
     unsigned device_error() const;  // syncs
+    const unsigned* device_error_ptr() const { return d_bar_ + 2; }
     void clear_error();
 
     // Full-tensor fields (row-major DxD per voxel) to host; syncs.

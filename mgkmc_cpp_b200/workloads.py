@@ -1,0 +1,109 @@
+"""Named benchmark / parity workloads, written in the reference's own input
+format (YAML keys of main.cpp and a ``.npy`` modulus field).
+
+No public dataset is involved: the heterogeneous cases use seeded synthetic
+lognormal modulus fields (``fields.lognormal_modulus``) with the shapes,
+correlation lengths and coefficients of variation of the benchmark cases.
+
+* ``homog2d_32``  -- 2D plane strain 32x32, E = 90 GPa, nu = 0.36, M = 18,
+  gamma0 = 0.1, barriers N(1.0, 0) (every Q0 = 1.0 eV), T = 300 K,
+  nu0 = 1e13 /s, strain rate 0.1 /s, sigma_yy = sigma_xy = 0, seed 0.
+* ``hetero2d_256`` -- 2D plane strain 256x256, lognormal E (mean 90 GPa,
+  CoV 0.10, correlation length 4 voxels), nu = 0.36, M = 18, Q0 per
+  (voxel, mode) ~ N(1.0, 0.1) clipped to [0.6, 1.4] eV, otherwise as above.
+* ``hetero2d_64``  -- the same at 64x64 (parity-test size).
+* ``hetero3d_64``  -- 3D 64^3, lognormal E (CoV 0.15, correlation 3), M = 100
+  random deviatoric 3D modes (system.3d_barriers), z tension.
+* ``hetero3d_16``  -- the 3D case at 16^3 with M = 20 (parity-test size).
+"""
+from __future__ import annotations
+
+import os
+from typing import Tuple
+
+import numpy as np
+
+from . import fields
+from .config import SimConfig, YAMLConfig
+
+_BASE = """
+seed: {seed}
+simulation_type: "kmc"
+system:
+  dimensionality: "{dim}"
+  plane_mode: "plane_strain"
+  nx: {nx}
+  ny: {ny}
+  nz: {nz}
+  pixel: 1.0
+  M: {M}
+  gamma0: 0.1
+  3d_barriers: {b3}
+material:
+  E:
+{Eblock}
+  nu:
+    mode: "constant"
+    value: 0.36
+loading:
+  eps_target: 0.05
+  step_size: 1e-4
+boundary_conditions:
+  driving_component: "{drive}"
+  mixed_targets:
+{targets}
+  mixed_tol: 1.0
+barriers:
+  type: "gaussian"
+  kwargs:
+    mean: 1.0
+    std: {bstd}
+    min_cutoff: 0.6
+    max_cutoff: 1.4
+physics:
+  enable_softening: false
+dynamics:
+  instability_mode: "cascade"
+  temperature: 300
+  nu0: 1e13
+  physical_strain_rate: 0.1
+output:
+  enable_console: false
+"""
+
+WORKLOADS = {
+    "homog2d_32": dict(dim="2d", nx=32, ny=32, nz=1, M=18, b3="false", hetero=None, drive="xx", bstd="0.0",
+                       targets="    yy: 0.0\n    xy: 0.0"),
+    "hetero2d_256": dict(dim="2d", nx=256, ny=256, nz=1, M=18, b3="false", hetero=(0.10, 4.0), drive="xx", bstd="0.1",
+                         targets="    yy: 0.0\n    xy: 0.0"),
+    "hetero2d_64": dict(dim="2d", nx=64, ny=64, nz=1, M=18, b3="false", hetero=(0.10, 4.0), drive="xx", bstd="0.1",
+                        targets="    yy: 0.0\n    xy: 0.0"),
+    "hetero3d_64": dict(dim="3d", nx=64, ny=64, nz=64, M=100, b3="true", hetero=(0.15, 3.0), drive="zz", bstd="0.1",
+                        targets="    xx: 0.0\n    yy: 0.0"),
+    "hetero3d_16": dict(dim="3d", nx=16, ny=16, nz=16, M=20, b3="true", hetero=(0.15, 3.0), drive="zz", bstd="0.1",
+                        targets="    xx: 0.0\n    yy: 0.0"),
+}
+
+
+def write_workload(name: str, directory: str, seed: int = 0) -> Tuple[str, SimConfig]:
+    """Writes <directory>/<name>_s<seed>.yaml (+ its E .npy) and returns (yaml_path, config)."""
+    w = WORKLOADS[name]
+    os.makedirs(directory, exist_ok=True)
+    if w["hetero"] is None:
+        eblock = '    mode: "constant"\n    value: 90'
+    else:
+        cov, corr = w["hetero"]
+        shape = (w["nx"], w["ny"], w["nz"]) if w["dim"] == "3d" else (w["nx"], w["ny"])
+        E = fields.lognormal_modulus(shape, 90e9, cov, corr, seed)
+        epath = os.path.join(directory, "E_%s_s%d.npy" % (name, seed))
+        np.save(epath, E)
+        eblock = '    mode: "file"\n    parameters:\n      path: "%s"' % epath
+    text = _BASE.format(seed=seed, Eblock=eblock, **{k: v for k, v in w.items() if k != "hetero"})
+    path = os.path.join(directory, "%s_s%d.yaml" % (name, seed))
+    with open(path, "w") as f:
+        f.write(text)
+    return path, SimConfig.from_yaml(path)
+
+
+def load_config(text: str) -> SimConfig:
+    return SimConfig.from_yaml(YAMLConfig.loads(text))

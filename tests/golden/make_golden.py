@@ -1,0 +1,189 @@
+#!/usr/bin/env python3
+"""Regenerates the golden fixtures in tests/golden/ from the reference itself.
+
+Every output comes from oracle/_ref/ref_driver, i.e. the unmodified mgkmc_cpp
+headers compiled by oracle/Makefile (run `make -C oracle` where the reference
+sources are present).  Inputs are seeded synthetic fields and small configs in
+the reference's YAML key surface; nothing is copied from the reference tree.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle as O  # noqa: E402
+
+# ------------------------------------------------------------------ LS cases
+LS_CASES = [
+    # name, dims, plane_mode, pixel, max_iter, tol, hetero, epsp, warm
+    ("ls2d_16_fixed3", (16, 16), "plane_strain", 1.0, 3, 0.0, True, True, False),
+    ("ls2d_16_conv", (16, 16), "plane_strain", 1.0, 200, 1e-6, True, True, False),
+    ("ls2d_12x10_stress_warm", (12, 10), "plane_stress", 0.5, 200, 1e-6, True, False, True),
+    ("ls2d_9x7_odd", (9, 7), "plane_strain", 1.0, 200, 1e-6, True, True, False),
+    ("ls2d_32_homog", (32, 32), "plane_strain", 1.0, 200, 1e-6, False, False, False),
+    ("ls2d_48x30_fixed2", (48, 30), "plane_strain", 1.0, 2, 0.0, True, True, True),
+    ("ls3d_8_fixed2", (8, 8, 8), "", 1.0, 2, 0.0, True, True, False),
+    ("ls3d_6x4x5_conv", (6, 4, 5), "", 0.7, 200, 1e-6, True, True, True),
+    ("ls3d_8x8x1_conv", (8, 8, 1), "", 1.0, 200, 1e-6, True, False, False),
+    ("ls3d_12x6x10_conv", (12, 6, 10), "", 1.0, 200, 1e-6, True, True, False),
+]
+
+
+def ls_inputs(name, dims, hetero, with_epsp, warm):
+    rng = np.random.default_rng(sum(map(ord, name)))
+    D = len(dims)
+    N = int(np.prod(dims))
+    E = 90e9 * (1 + 0.2 * rng.standard_normal(N)) if hetero else np.full(N, 90e9)
+    nu = np.full(N, 0.36) if hetero else np.full(N, 0.3)
+    eb = 1e-3 * rng.standard_normal((D, D))
+    epsp = None
+    if with_epsp:
+        epsp = 0.01 * rng.standard_normal((N, D, D))
+        epsp = epsp + epsp.transpose(0, 2, 1)
+    eps0 = 1e-3 * rng.standard_normal((N, D, D)) if warm else None
+    return E, nu, eb, epsp, eps0
+
+
+# ------------------------------------------------------------------ KMC cases
+KMC_YAML = """
+seed: {seed}
+system:
+  dimensionality: "{dim}"
+  plane_mode: "{plane}"
+  nx: {nx}
+  ny: {ny}
+  nz: {nz}
+  pixel: {pixel}
+  M: {M}
+  gamma0: 0.1
+  3d_barriers: {b3}
+material:
+  E:
+{Eblock}
+  nu:
+    mode: "constant"
+    value: 0.36
+loading:
+  eps_target: 0.05
+  step_size: 1e-3
+boundary_conditions:
+  driving_component: "{drive}"
+  mixed_targets:
+{targets}
+  mixed_tol: 1.0
+barriers:
+  type: "{btype}"
+  kwargs:
+    mean: 1.0
+    std: 0.1
+    min_cutoff: 0.6
+    max_cutoff: 1.4
+    loc: 0.7
+    scale: 0.2
+    epsilon: 0.3
+    ratio: 0.5
+physics:
+  enable_softening: {soft}
+  softening_scheme: "{scheme}"
+  neighbor_softening_fraction: {neigh}
+  jp: 1.0
+  jt: 3.0
+  softening_cap: 0.5
+  q_act_temp: 0.6
+  redraw_directions: {rdir}
+  redraw_barriers: {rbar}
+dynamics:
+  instability_mode: "{mode}"
+  temperature: 300
+  nu0: 1e13
+  physical_strain_rate: 0.1
+"""
+
+_K = dict(seed=3, dim="2d", plane="plane_strain", nx=12, ny=12, nz=1, pixel=1.0, M=6, b3="false", hetero=False,
+          drive="xx", targets="    yy: 0.0\n    xy: 0.0", btype="gaussian", soft="false", scheme="isotropic", neigh=0.0,
+          rdir="true", rbar="true", mode="cascade", nsteps=25, maxev=300)
+
+KMC_CASES = {
+    "kmc2d_12_nosoft": dict(),
+    "kmc2d_8_soft_neigh": dict(nx=8, ny=8, M=5, soft="true", neigh=0.1),
+    "kmc2d_8_kmcmode": dict(nx=8, ny=8, M=4, soft="true", neigh=0.1, mode="kmc"),
+    "kmc2d_10_hetero_stress": dict(nx=10, ny=10, M=4, plane="plane_stress", hetero=True, btype="modified_rayleigh",
+                                   soft="true", scheme="directional", pixel=0.8, seed=5),
+    "kmc2d_8_noredraw": dict(nx=8, ny=6, M=3, rdir="false", rbar="false", btype="rayleigh", drive="xy",
+                             targets="    xx: 0.0\n    yy: 0.0", seed=11),
+    "kmc2d_8_mixexp": dict(nx=8, ny=8, M=4, btype="modified_rayleigh_with_exponential", rbar="false", seed=13),
+    "kmc3d_6x6x4_soft": dict(dim="3d", nx=6, ny=6, nz=4, M=4, soft="true", neigh=0.1),
+    "kmc3d_5x4x3_b3dir": dict(dim="3d", nx=5, ny=4, nz=3, M=3, b3="true", soft="true", scheme="directional",
+                              drive="zz", targets="    xx: 0.0\n    yy: 0.0", hetero=True, seed=7),
+}
+
+
+def kmc_yaml(name, epath=None):
+    k = dict(_K)
+    k.update(KMC_CASES[name])
+    if k["hetero"]:
+        eblock = '    mode: "file"\n    parameters:\n      path: "%s"' % (epath or "$E")
+    else:
+        eblock = '    mode: "constant"\n    value: 90'
+    return KMC_YAML.format(Eblock=eblock, **k), k
+
+
+def kmc_field(name):
+    k = dict(_K)
+    k.update(KMC_CASES[name])
+    if not k["hetero"]:
+        return None
+    shape = (k["nx"], k["ny"], k["nz"]) if k["dim"] == "3d" else (k["nx"], k["ny"])
+    rng = np.random.default_rng(sum(map(ord, name)))
+    return 90.0 * np.exp(0.15 * rng.standard_normal(shape))  # GPa; the reader converts to Pa
+
+
+def main():
+    rd = O.RefDriver()
+    # RNG draws
+    with tempfile.TemporaryDirectory() as d:
+        subprocess.run([rd.path, "draws", "7", "200", d + "/x.npy"], check=True)
+        np.savez_compressed(os.path.join(HERE, "draws_seed7.npz"), draws=np.load(d + "/x.npy"))
+    # LS
+    for (name, dims, pm, pixel, it, tol, het, wep, warm) in LS_CASES:
+        E, nu, eb, epsp, eps0 = ls_inputs(name, dims, het, wep, warm)
+        D = len(dims)
+        N = int(np.prod(dims))
+        eps, sig, em, sm, _ = rd.ls(dims, E, nu, eb, eps0=None if eps0 is None else eps0.reshape(N, D * D),
+                                    epsp=None if epsp is None else epsp.reshape(N, D * D),
+                                    plane_mode=pm or "plane_strain", pixel=pixel, max_iter=it, tol=tol)
+        arrs = dict(dims=np.array(dims), E=E, nu=nu, eps_bar=eb, pixel=pixel, max_iter=it, tol=tol,
+                    plane_stress=int(pm == "plane_stress"), eps=eps, sig=sig, eps_macro=em, sig_macro=sm)
+        if epsp is not None:
+            arrs["epsp"] = epsp.reshape(N, D * D)
+        if eps0 is not None:
+            arrs["eps0"] = eps0.reshape(N, D * D)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
+        print("wrote", name)
+    # KMC traces
+    for name in KMC_CASES:
+        y, k = kmc_yaml(name, "$DIR/E.npy")
+        Ef = kmc_field(name)
+        files = {"E.npy": Ef} if Ef is not None else {}
+        res = rd.kmc(y, "kmc_trace", nsteps=k["nsteps"], maxev=k["maxev"], files=files)
+        arrs = {f: res[f] for f in ("trace", "eps", "sig", "epsp", "catalog", "Q0", "soft", "prev_dir", "macro", "last_t")}
+        arrs["yaml"] = np.array(kmc_yaml(name, "$E")[0])
+        if Ef is not None:
+            arrs["E_gpa"] = Ef
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
+        print("wrote", name, "rows", len(res["trace"]), "kinds", np.bincount(res["trace"][:, 0].astype(int)))
+
+
+if __name__ == "__main__":
+    main()

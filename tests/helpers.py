@@ -1,0 +1,58 @@
+"""Shared helpers for the test suite (fixture loading, comparisons)."""
+import os
+import tempfile
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def rel(a, b):
+    a, b = np.ravel(a), np.ravel(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def kmc_config_from_golden(g):
+    """SimConfig of a golden KMC case (writes its modulus field to a temp file)."""
+    from mgkmc_cpp_b200.config import SimConfig, YAMLConfig
+    y = str(g["yaml"])
+    if "E_gpa" in g:
+        d = tempfile.mkdtemp()
+        p = os.path.join(d, "E.npy")
+        np.save(p, g["E_gpa"])
+        y = y.replace("$E", p)
+    return SimConfig.from_yaml(YAMLConfig.loads(y)), y
+
+
+KMC_CASES = ["kmc2d_12_nosoft", "kmc2d_8_soft_neigh", "kmc2d_8_kmcmode", "kmc2d_10_hetero_stress", "kmc2d_8_noredraw",
+             "kmc2d_8_mixexp", "kmc3d_6x6x4_soft", "kmc3d_5x4x3_b3dir"]
+LS_CASES = ["ls2d_16_fixed3", "ls2d_16_conv", "ls2d_12x10_stress_warm", "ls2d_9x7_odd", "ls2d_32_homog",
+            "ls2d_48x30_fixed2", "ls3d_8_fixed2", "ls3d_6x4x5_conv", "ls3d_8x8x1_conv", "ls3d_12x6x10_conv"]
+KMC_RUN = {"kmc2d_12_nosoft": (25, 300), "kmc2d_8_soft_neigh": (25, 300), "kmc2d_8_kmcmode": (25, 300),
+           "kmc2d_10_hetero_stress": (25, 300), "kmc2d_8_noredraw": (25, 300), "kmc2d_8_mixexp": (25, 300),
+           "kmc3d_6x6x4_soft": (25, 300), "kmc3d_5x4x3_b3dir": (25, 300)}
+
+
+def compare_trace(tr, ref, tol=1e-9):
+    """Kinds, selected indices and counters must be identical; the continuous
+    columns (total rate, wait, clock, macro tensors) within `tol` relative to
+    each column's scale."""
+    assert tr.shape == ref.shape, (tr.shape, ref.shape)
+    kind = ref[:, 0]
+    assert np.array_equal(tr[:, 0], kind)
+    ev = kind != 2  # column 1 of an interval-end row is the u1 draw (float)
+    assert np.array_equal(tr[ev, 1], ref[ev, 1])
+    assert np.array_equal(tr[:, 2], ref[:, 2])
+    DD = (ref.shape[1] - 6) // 2
+    scale = np.abs(ref[:, 3:]).max(axis=0) + 1e-300
+    # tensor columns share one scale per tensor (components that are zero in
+    # exact arithmetic carry only rounding noise)
+    scale[3:3 + DD] = scale[3:3 + DD].max()
+    scale[3 + DD:] = scale[3 + DD:].max()
+    err = np.abs(tr[:, 3:] - ref[:, 3:]) / scale
+    assert err.max() <= tol, (err.max(), np.unravel_index(np.argmax(err), err.shape))
+    assert np.allclose(tr[~ev, 1], ref[~ev, 1], rtol=0, atol=0)
