@@ -100,6 +100,7 @@ typedef struct {
     int enable_summary_log, enable_global_log, enable_console;
     const char* vtk_interval; /* "none" | "last" | "current" | "<int>" */
     int vtk_elastic_only;
+    long long max_cascade_batches; /* <= 0: the reference's limit, N batches (kmc_solver.hpp:467, 556) */
 } mgk_run_params;
 
 typedef struct mgk_kmc mgk_kmc;

@@ -169,7 +169,7 @@ class _KmcBase:
                        mixed_tol=1e-4, mixed_max_iter=50, checkpoint_interval="none", checkpoint_path="checkpoint",
                        vtk_interval="none", vtk_elastic_only=True, track_cascades=False, enable_console_log=True,
                        summary_filename="summary_log.txt", enable_summary_log=True, enable_global_log=True,
-                       max_kmc_steps_pct=0.3, max_events=0, trace=False, trace_cap=1 << 20):
+                       max_kmc_steps_pct=0.3, max_events=0, trace=False, trace_cap=1 << 20, max_cascade_batches=0):
         """kmc_solver.hpp:721-1037.  Returns the event trace (rows of
         [kind, a, b, total_rate, t_wait, time, eps_macro, sig_macro]) when
         ``trace`` is true, else None.  Raises MgkError on failure; the
@@ -183,6 +183,7 @@ class _KmcBase:
             rp.target_i[k], rp.target_j[k], rp.target_v[k] = i, j, v
         rp.mixed_tol, rp.mixed_max_iter, rp.max_kmc_steps_pct = mixed_tol, int(mixed_max_iter), max_kmc_steps_pct
         rp.max_events = int(max_events or 0)
+        rp.max_cascade_batches = int(max_cascade_batches or 0)
         out = self.output_dir if (enable_summary_log or enable_global_log or vtk_interval != "none") else None
         if out:
             os.makedirs(out, exist_ok=True)

@@ -46,7 +46,8 @@ class RunParamsC(C.Structure):
                 ("target_v", C.c_double * 9), ("mixed_tol", C.c_double), ("mixed_max_iter", C.c_int),
                 ("max_kmc_steps_pct", C.c_double), ("max_events", C.c_longlong), ("output_dir", C.c_char_p),
                 ("summary_filename", C.c_char_p), ("enable_summary_log", C.c_int), ("enable_global_log", C.c_int),
-                ("enable_console", C.c_int), ("vtk_interval", C.c_char_p), ("vtk_elastic_only", C.c_int)]
+                ("enable_console", C.c_int), ("vtk_interval", C.c_char_p), ("vtk_elastic_only", C.c_int),
+                ("max_cascade_batches", C.c_longlong)]
 
 
 _lib = None

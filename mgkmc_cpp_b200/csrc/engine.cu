@@ -9,6 +9,7 @@
 // enqueues select+flip, the warm-started LS solve and the next sweep in one go.
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <ctime>
 #include <limits>
@@ -77,6 +78,18 @@ double BarrierGen::generate(std::mt19937& rng) const {
     } while (0)
 
 static const double kB = 8.617e-5;
+
+// Opt-in host-side trace of the run loop (environment MGK_DEBUG=<max lines>).
+static long g_debug_left = -1;
+static bool dbg() {
+    if (g_debug_left < 0) {
+        const char* e = std::getenv("MGK_DEBUG");
+        g_debug_left = e ? std::atol(e) : 0;
+    }
+    if (g_debug_left <= 0) return false;
+    --g_debug_left;
+    return true;
+}
 
 KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu) : p_(p), rng_((unsigned)p.seed) {
     if (p.dim != 2 && p.dim != 3) throw std::invalid_argument("dim must be 2 or 3");
@@ -383,9 +396,9 @@ mgk_status KmcEngine::elastic_run() {
 
 // run_cascade (kmc_solver.hpp:464-564): entered with a fresh sweep in
 // h_status_ that found unstable modes.
-mgk_status KmcEngine::run_cascade(int* steps, int* flips) {
+mgk_status KmcEngine::run_cascade(int* steps, int* flips, long long cap) {
     int total = 0, local = 0;
-    const int limit = N_;
+    const long long limit = cap > 0 ? cap : (long long)N_;
     const size_t rec = (size_t)((p_.redraw_directions || p_.redraw_barriers) ? M_ : 1) * (C_ + 1);
     while (true) {
         if (h_status_->n_unstable == 0) break;
@@ -397,6 +410,7 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips) {
         CK(cudaStreamSynchronize(st_));
         stats_.syncs++;
         const int n = h_status_->n_collect;
+        if (dbg()) fprintf(stderr, "[mgk] cascade collect: n_unstable %d collected %d\n", h_status_->n_unstable, n);
         if (n <= 0) break;
         // draws of the n flips in flip order (one normal object per flip)
         const size_t need = (size_t)n * rec;
@@ -419,6 +433,7 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips) {
             stats_.launches += 1 + (np2 <= 8192 ? 1 : 1 + lg * (lg + 1) / 2);
         }
         CK(enqueue_elastic());
+        if (dbg()) fprintf(stderr, "[mgk] cascade batch %d flips %d\n", local, n);
         total += n;
         ++local;
         CK(enqueue_sweep());
@@ -569,6 +584,7 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
     };
     int elastic_done = 0, total_kmc = 0, step = 1, seq_instab = 0;
     const long long events_at_start = stats_.thermal_events;
+    g_debug_left = -1;  // re-read MGK_DEBUG for this run
     const int max_seq = (int)(rp.max_kmc_steps_pct * (double)N_);
     mgk_status s;
     try {
@@ -576,6 +592,7 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
         CK(enqueue_elastic());
         CK(enqueue_sweep());
         s = sync_status();
+        if (dbg()) fprintf(stderr, "[mgk] run start: LS iters %d, n_unstable %d, status %d\n", h_lsres_->iters, h_status_->n_unstable, (int)s);
         if (s != MGK_OK) return s;
         if (console_) {
             fputs("Timestamp              Elapsed(s)   Step     Type            Eps_xx       Sig_xx(GPa)     KMC      Cascade  Flips    SimTime(s)\n", stdout);
@@ -593,7 +610,7 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                 // h_status_ holds the sweep of the current state (update_barriers)
                 if (!p_.instability_kmc && h_status_->n_unstable > 0) {
                     int cs = 0, cf = 0;
-                    s = run_cascade(&cs, &cf);
+                    s = run_cascade(&cs, &cf, rp.max_cascade_batches);
                     if (s != MGK_OK) {
                         close_logs();
                         return s;
@@ -608,6 +625,9 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                 }
                 const double R = h_status_->total_hi + h_status_->total_lo;
                 const double t_ev = wall_seconds();
+                if (dbg())
+                    fprintf(stderr, "[mgk] loop R=%.6e remaining=%.6e n_unstable=%d events=%lld time=%.9e\n", R, remaining,
+                            h_status_->n_unstable, stats_.thermal_events, time_);
                 if (R > 0.0) {
                     const double u1 = U(rng_);
                     const double tw = -std::log(u1) / R;
@@ -668,8 +688,10 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
             for (double v : nu_) ns += v;
             const double Ea = Es / E_.size(), na = ns / nu_.size();
             int solves = 0;
+            if (dbg()) fprintf(stderr, "[mgk] mixed-BC loop, elastic step %d\n", elastic_done + 1);
             for (int it = 0; it < rp.mixed_max_iter; ++it) {
                 s = elastic_run();
+                if (dbg()) fprintf(stderr, "[mgk]   mixed it %d iters %d sig_macro %.6e %.6e\n", it, h_lsres_->iters, sig_macro_[0], sig_macro_[D * D - 1]);
                 if (s != MGK_OK) {
                     close_logs();
                     return s;

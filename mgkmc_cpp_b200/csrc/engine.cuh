@@ -64,7 +64,7 @@ private:
     mgk_status sync_status();  // waits for the stream, copies status + LS result
     void gen_flip_draws(double* out);
     void draw_mode(std::normal_distribution<double>& sn, double* out);
-    mgk_status run_cascade(int* steps, int* flips);
+    mgk_status run_cascade(int* steps, int* flips, long long cap);
     void log_line(int global_step, int elastic_steps_done, int total_kmc, const char* type, int csteps, int cflips);
     void maybe_vtk(int global_step, int elastic_steps_done, const char* type, bool init);
     void export_vtu(const std::string& name);

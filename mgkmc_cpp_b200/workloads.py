@@ -10,8 +10,13 @@ correlation lengths and coefficients of variation of the benchmark cases.
   nu0 = 1e13 /s, strain rate 0.1 /s, sigma_yy = sigma_xy = 0, seed 0.
 * ``hetero2d_256`` -- 2D plane strain 256x256, lognormal E (mean 90 GPa,
   CoV 0.10, correlation length 4 voxels), nu = 0.36, M = 18, Q0 per
-  (voxel, mode) ~ N(1.0, 0.1) clipped to [0.6, 1.4] eV, otherwise as above.
-* ``hetero2d_64``  -- the same at 64x64 (parity-test size).
+  (voxel, mode) from the reference's default barrier generator (N(2.0, 0.6)
+  eV, cut off below 0.1 eV), otherwise as above.
+* ``hetero2d_256_dF1`` -- the same with Q0 ~ N(1.0, 0.1) clipped to
+  [0.6, 1.4] eV per (voxel, mode).  In the reference's model this enters a
+  sustained avalanche after about 1100 thermal events at seed 0 (the cascade
+  loop never settles), in the reference and in this build alike.
+* ``hetero2d_64``  -- 64x64 with the N(1.0, 0.1) barriers (parity-test size).
 * ``hetero3d_64``  -- 3D 64^3, lognormal E (CoV 0.15, correlation 3), M = 100
   random deviatoric 3D modes (system.3d_barriers), z tension.
 * ``hetero3d_16``  -- the 3D case at 16^3 with M = 20 (parity-test size).
@@ -56,10 +61,10 @@ boundary_conditions:
 barriers:
   type: "gaussian"
   kwargs:
-    mean: 1.0
+    mean: {bmean}
     std: {bstd}
-    min_cutoff: 0.6
-    max_cutoff: 1.4
+    min_cutoff: {bmin}
+    max_cutoff: {bmax}
 physics:
   enable_softening: false
 dynamics:
@@ -71,17 +76,22 @@ output:
   enable_console: false
 """
 
+# barrier distributions: the reference's BarrierGenerator defaults
+# (gaussian, mean 2.0 eV, std 0.6, min cutoff 0.1, main.cpp:283-286) and the
+# N(1.0, 0.1) eV clipped to [0.6, 1.4] distribution of the heterogeneous cases
+_B_REF = dict(bmean="2.0", bstd="0.6", bmin="0.1", bmax="-1.0")
+_B_DF1 = dict(bmean="1.0", bstd="0.1", bmin="0.6", bmax="1.4")
+_T2 = dict(drive="xx", targets="    yy: 0.0\n    xy: 0.0")
+_T3 = dict(drive="zz", targets="    xx: 0.0\n    yy: 0.0")
+
 WORKLOADS = {
-    "homog2d_32": dict(dim="2d", nx=32, ny=32, nz=1, M=18, b3="false", hetero=None, drive="xx", bstd="0.0",
-                       targets="    yy: 0.0\n    xy: 0.0"),
-    "hetero2d_256": dict(dim="2d", nx=256, ny=256, nz=1, M=18, b3="false", hetero=(0.10, 4.0), drive="xx", bstd="0.1",
-                         targets="    yy: 0.0\n    xy: 0.0"),
-    "hetero2d_64": dict(dim="2d", nx=64, ny=64, nz=1, M=18, b3="false", hetero=(0.10, 4.0), drive="xx", bstd="0.1",
-                        targets="    yy: 0.0\n    xy: 0.0"),
-    "hetero3d_64": dict(dim="3d", nx=64, ny=64, nz=64, M=100, b3="true", hetero=(0.15, 3.0), drive="zz", bstd="0.1",
-                        targets="    xx: 0.0\n    yy: 0.0"),
-    "hetero3d_16": dict(dim="3d", nx=16, ny=16, nz=16, M=20, b3="true", hetero=(0.15, 3.0), drive="zz", bstd="0.1",
-                        targets="    xx: 0.0\n    yy: 0.0"),
+    "homog2d_32": dict(dim="2d", nx=32, ny=32, nz=1, M=18, b3="false", hetero=None, **_T2, bmean="1.0", bstd="0.0",
+                       bmin="0.6", bmax="1.4"),
+    "hetero2d_256": dict(dim="2d", nx=256, ny=256, nz=1, M=18, b3="false", hetero=(0.10, 4.0), **_T2, **_B_REF),
+    "hetero2d_256_dF1": dict(dim="2d", nx=256, ny=256, nz=1, M=18, b3="false", hetero=(0.10, 4.0), **_T2, **_B_DF1),
+    "hetero2d_64": dict(dim="2d", nx=64, ny=64, nz=1, M=18, b3="false", hetero=(0.10, 4.0), **_T2, **_B_DF1),
+    "hetero3d_64": dict(dim="3d", nx=64, ny=64, nz=64, M=100, b3="true", hetero=(0.15, 3.0), **_T3, **_B_REF),
+    "hetero3d_16": dict(dim="3d", nx=16, ny=16, nz=16, M=20, b3="true", hetero=(0.15, 3.0), **_T3, **_B_DF1),
 }
 
 
