@@ -61,6 +61,35 @@ MGK_API mgk_status mgk_ls_solve(mgk_ls* h, const double* eps_bar, const double* 
                         double* sig_out, double* macro_out, int max_iter, double tol, int* iters_out);
 MGK_API void mgk_ls_destroy(mgk_ls* h);
 
+/* ---------------------------------------------------------------- LS solve without allocating
+ * No counterpart in the reference.  One LS solve like mgk_ls_solve, for
+ * callers that may not allocate device memory: a host application that has
+ * reserved the GPU's memory for its own pool (another cudaMalloc would fail or
+ * fragment it), or a loop that cannot pay for cudaMalloc/cudaFree, which
+ * synchronise the whole device.  The caller passes DEVICE buffers:
+ * E_dev, nu_dev (N values), eps_plastic_dev (N*D*D or NULL), eps_dev (N*D*D,
+ * read as the warm start when warm != 0, written with the solution) and
+ * sig_dev (N*D*D or NULL); eps_bar (D*D), macro_out (2*D*D or NULL) and
+ * iters_out are host pointers; stream is a cudaStream_t (NULL: the legacy
+ * default stream).  The call returns after the stream has finished the solve.
+ * Nothing is allocated: every intermediate lives in one static device array of
+ * MGK_NOALLOC_SCRATCH_BYTES (16 MiB), which every GPU that loads the library
+ * holds until the process exits; grids whose intermediates exceed it (about
+ * 88 bytes per voxel in 2D, 170 in 3D; e.g. up to 256x256 in 2D or 40^3 in
+ * 3D) are refused with MGK_BAD_SHAPE.  The first call on a device looks up the
+ * array's device address (and may load the library's GPU code), so make that
+ * first call before any stream capture.  All calls share the one array, which
+ * keeps the previous call's contents (each call resets what must start at
+ * zero): calls that overlap on the GPU, from several streams or threads, race
+ * and must be serialised by the caller.  mgk_noalloc_last_error() describes
+ * the last failure of this entry point on the calling thread. */
+#define MGK_NOALLOC_SCRATCH_BYTES (16u << 20)
+MGK_API mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stress, double pixel, const double* E_dev,
+                                        const double* nu_dev, const double* eps_bar, const double* eps_plastic_dev,
+                                        double* eps_dev, int warm, double* sig_dev, double* macro_out, int max_iter, double tol,
+                                        int* iters_out, void* stream);
+MGK_API const char* mgk_noalloc_last_error(void);
+
 /* ---------------------------------------------------------------- KMC
  * Replaces the KmcSimulation2D constructor (kmc_solver.hpp:165-182) and the
  * KmcSimulation3D constructor (:1142-1158): the same parameters, in one struct. */

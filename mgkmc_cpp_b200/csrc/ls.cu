@@ -19,10 +19,15 @@
 //    and is not repeated here;
 //  * the symmetric part of eps is stored; the antisymmetric part is uniform
 //    (it only ever comes from eps_bar) and is carried as three scalars.
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
+#include <string>
 
+#include "../../include/mgkmc_b200.h"
 #include "ls.cuh"
 
 namespace mgk {
@@ -725,3 +730,293 @@ cudaError_t LsSolver::upload_eps(const double* host) {
 }
 
 }  // namespace mgk
+
+// ---------------------------------------------------------------------------
+// Solve without allocating: mgk_ls_solve_noalloc (declared in mgkmc_b200.h).
+//
+// For callers that must not allocate device memory themselves or through this
+// library: host applications that reserve the whole GPU for their own memory
+// pool (a further cudaMalloc fails or fragments it), and loops that cannot
+// afford cudaMalloc/cudaFree, which synchronise the device.  They hand in
+// device buffers for the inputs and outputs; every intermediate (strain
+// components, moduli, spectrum, twiddles, reduction partials, barrier words)
+// lives in one static device array of MGK_NOALLOC_SCRATCH_BYTES that the
+// library holds on every GPU it is loaded on, until the process exits.
+namespace mgk {
+namespace {
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[MGK_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on the current device.  In host code the
+// symbol g_noalloc_scratch only names a host-side stand-in, so it is never
+// passed to a kernel; the address comes from cudaGetSymbolAddress, looked up
+// once per device with that device current.
+cudaError_t noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+// One CTA: sums of E, nu, mu and of the antisymmetric parts of eps (fixed order).
+template <int D>
+__global__ void noalloc_prep_kernel(const double* __restrict__ E, const double* __restrict__ nu, const double* __restrict__ eps,
+                                    int N, int warm, double* __restrict__ out) {
+    constexpr int NO = D == 2 ? 1 : 3;
+    double v[3 + 2 * NO];
+#pragma unroll
+    for (int k = 0; k < 3 + 2 * NO; ++k) v[k] = 0.0;
+    const int pi[3] = {0, 0, 1}, pj[3] = {1, 2, 2};
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        v[0] += E[i];
+        v[1] += nu[i];
+        v[2] += E[i] / (2.0 * (1.0 + nu[i]));
+        if (warm)
+#pragma unroll
+            for (int k = 0; k < NO; ++k) {
+                const double a = 0.5 * (eps[(long)i * D * D + pi[k] * D + pj[k]] - eps[(long)i * D * D + pj[k] * D + pi[k]]);
+                v[3 + k] += a;
+                v[3 + NO + k] += a * a;
+            }
+    }
+    __shared__ double scratch[(3 + 2 * NO) * 32];
+    block_sum<3 + 2 * NO>(v, scratch);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 3 + 2 * NO; ++k) out[k] = v[k];
+}
+
+__global__ void noalloc_moduli_kernel(const double* __restrict__ E, const double* __restrict__ nu, int N, int D, int ps,
+                                      double* __restrict__ lam, double* __restrict__ mu) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+        mu[i] = E[i] / (2.0 * (1.0 + nu[i]));
+        lam[i] = (D == 2 && ps) ? E[i] * nu[i] / (1.0 - nu[i] * nu[i]) : E[i] * nu[i] / ((1.0 + nu[i]) * (1.0 - 2.0 * nu[i]));
+    }
+}
+
+__global__ void noalloc_twiddle_kernel(int n, cplx<double>* tw64, cplx<float>* tw32) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        double s, c;
+        sincospi(-2.0 * (double)k / (double)n, &s, &c);
+        tw64[k] = {c, s};
+        tw32[k] = {(float)c, (float)s};
+    }
+}
+
+bool noalloc_radices(int n, FftAxis* ax) {
+    std::memset(ax, 0, sizeof(*ax));
+    ax->n = n;
+    int m = n, k = 0;
+    while (m % 8 == 0 && m >= 64 && k < kMaxStages) { ax->radix[k++] = 8; m /= 8; }
+    while (m % 4 == 0 && k < kMaxStages) { ax->radix[k++] = 4; m /= 4; }
+    static const int primes[] = {2, 3, 5, 7, 11, 13};
+    for (int p : primes)
+        while (m % p == 0 && k < kMaxStages) { ax->radix[k++] = p; m /= p; }
+    ax->nst = k;
+    return m == 1;
+}
+
+}  // namespace
+}  // namespace mgk
+
+namespace {
+thread_local std::string g_noalloc_err;
+mgk_status noalloc_fail(mgk_status s, const std::string& m) {
+    g_noalloc_err = m;
+    return s;
+}
+}  // namespace
+
+const char* mgk_noalloc_last_error(void) { return g_noalloc_err.c_str(); }
+
+mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stress, double pixel, const double* E_dev,
+                                const double* nu_dev, const double* eps_bar, const double* eps_plastic_dev, double* eps_dev,
+                                int warm, double* sig_dev, double* macro_out, int max_iter, double tol, int* iters_out,
+                                void* stream) {
+    using namespace mgk;
+    if (!E_dev || !nu_dev || !eps_bar || !eps_dev) return noalloc_fail(MGK_BAD_ARG, "null argument");
+    if (dim != 2 && dim != 3) return noalloc_fail(MGK_BAD_SHAPE, "dim must be 2 or 3");
+    if (nx < 1 || ny < 1 || (dim == 3 && nz < 1)) return noalloc_fail(MGK_BAD_SHAPE, "grid sizes must be positive");
+    if (max_iter < 0) return noalloc_fail(MGK_BAD_ARG, "max_iter < 0");
+    const int D = dim, S = n_sym(D), DD = D * D;
+    const int dims[3] = {nx, ny, D == 3 ? nz : 1};
+    const long N = (long)dims[0] * dims[1] * dims[2];
+    const int nr = dims[D - 1], nh = nr / 2 + 1;
+    const long nrows = N / nr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    LsArgs a{};
+    a.D = D;
+    a.S = S;
+    for (int i = 0; i < 3; ++i) a.dims[i] = dims[i];
+    a.nr = nr;
+    a.nh = nh;
+    for (int i = 0; i < D; ++i)
+        if (!noalloc_radices(dims[i], &a.ax[i])) return noalloc_fail(MGK_BAD_SHAPE, "unsupported FFT length (prime factor > 13)");
+    // decomposition: the same rules as LsSolver
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    a.rpb = (S == 3) ? 2 : 1;
+    if (nrows / a.rpb < nsm / 2 && a.rpb > 1) a.rpb = 1;
+    const int no = (D == 2) ? 1 : std::max(dims[0], dims[1]);
+    a.tk = ((long)no * nh >= 4L * nsm) ? 2 : 1;
+    const long row_items = (nrows + a.rpb - 1) / a.rpb;
+    const long col_items = (long)((D == 2) ? 1 : std::min(dims[0], dims[1])) * ((nh + a.tk - 1) / a.tk);
+    const size_t elem = sizeof(cplx<double>);
+    const size_t row_b = (size_t)((a.rpb * S + 1) / 2) * nr * elem;
+    size_t col_b = 0;
+    for (int ax = 0; ax < D - 1; ++ax) col_b = std::max(col_b, (size_t)S * a.tk * dims[ax] * elem);
+    const size_t half_b = (std::max(row_b, col_b) + 127) / 128 * 128;
+    const size_t smem = 2 * half_b;
+    a.smem_half = (int)half_b;
+    if (smem > 200 * 1024) return noalloc_fail(MGK_BAD_SHAPE, "grid axis too long for the shared-memory FFT");
+    auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
+    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return noalloc_fail(MGK_CUDA_ERROR, "cannot configure the LS kernel");
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, 256, smem) != cudaSuccess || per_sm < 1)
+        return noalloc_fail(MGK_CUDA_ERROR, "LS kernel does not fit on an SM");
+    const int grid = (int)std::max(1L, std::min(std::max(row_items, col_items), (long)per_sm * nsm));
+    // carve the static scratch array
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off = (off + bytes + 255) / 256 * 256;
+        return o;
+    };
+    const size_t o_bar = take(4 * sizeof(unsigned)), o_res = take(sizeof(LsResult)), o_sum = take(16 * sizeof(double));
+    const size_t o_part = take(sizeof(double) * kMaxPartials * grid);
+    size_t o_tw64[3] = {0, 0, 0}, o_tw32[3] = {0, 0, 0};
+    for (int i = 0; i < D; ++i) {
+        o_tw64[i] = take(sizeof(cplx<double>) * dims[i]);
+        o_tw32[i] = take(sizeof(cplx<float>) * dims[i]);
+    }
+    const size_t o_lam = take(sizeof(double) * N), o_mu = take(sizeof(double) * N), o_eps = take(sizeof(double) * S * N);
+    const size_t o_epsp = eps_plastic_dev ? take(sizeof(double) * S * N) : 0;
+    const size_t o_spec = take(elem * S * (size_t)nrows * nh);
+    if (off > (size_t)MGK_NOALLOC_SCRATCH_BYTES) {
+        char msg[160];
+        snprintf(msg, sizeof(msg), "grid needs %zu scratch bytes, above the %u-byte static limit", off,
+                 (unsigned)MGK_NOALLOC_SCRATCH_BYTES);
+        return noalloc_fail(MGK_BAD_SHAPE, msg);
+    }
+    unsigned char* base = nullptr;
+    cudaError_t e = noalloc_scratch(&base);
+    if (e != cudaSuccess) return noalloc_fail(MGK_CUDA_ERROR, std::string("scratch lookup: ") + cudaGetErrorString(e));
+    double* sums = reinterpret_cast<double*>(base + o_sum);
+    double* lam = reinterpret_cast<double*>(base + o_lam);
+    double* mu = reinterpret_cast<double*>(base + o_mu);
+    double* eps_s = reinterpret_cast<double*>(base + o_eps);
+    double* epsp_s = eps_plastic_dev ? reinterpret_cast<double*>(base + o_epsp) : nullptr;
+    // sums for the reference medium and the antisymmetric part of the warm start
+    if (D == 2) noalloc_prep_kernel<2><<<1, 1024, 0, st>>>(E_dev, nu_dev, eps_dev, (int)N, warm, sums);
+    else noalloc_prep_kernel<3><<<1, 1024, 0, st>>>(E_dev, nu_dev, eps_dev, (int)N, warm, sums);
+    double hs[9] = {0};
+    e = cudaMemcpyAsync(hs, sums, sizeof(double) * 9, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return noalloc_fail(MGK_CUDA_ERROR, cudaGetErrorString(e));
+    double lam0, mu0;
+    lame(hs[0] / N, hs[1] / N, D, plane_stress != 0, &lam0, &mu0);
+    const double sum_two_mu = 2.0 * hs[2];
+    a.N = (int)N;
+    a.nrows = (int)nrows;
+    a.inv_n = 1.0 / (double)N;
+    a.lam0 = lam0;
+    a.mu0 = mu0;
+    a.inv2mu0 = 1.0 / (2.0 * mu0);
+    a.bcoef = (lam0 + mu0) / (mu0 * (lam0 + 2.0 * mu0));
+    a.pixel = pixel;
+    const int noff = D == 2 ? 1 : 3;
+    double wbar[3] = {0, 0, 0};
+    for (int i = 0; i < D; ++i)
+        for (int j = i; j < D; ++j) {
+            const int c = sym_idx(D, i, j);
+            a.ebar_s[c] = (i == j) ? eps_bar[i * D + i] : 0.5 * (eps_bar[i * D + j] + eps_bar[j * D + i]);
+            if (i != j) wbar[(D == 2) ? 0 : (i + j - 1)] = 0.5 * (eps_bar[i * D + j] - eps_bar[j * D + i]);
+        }
+    double sw2 = 0.0, sdev = 0.0;
+    for (int k = 0; k < noff; ++k) {
+        sw2 += wbar[k] * wbar[k];
+        if (warm) {
+            const double m = hs[3 + k] / N;
+            sdev += std::max(0.0, hs[3 + noff + k] - N * m * m);
+        }
+    }
+    a.norm_extra = 2.0 * (double)N * sw2;
+    a.norm_extra_first = warm ? 2.0 * (sdev + (double)N * sw2) : a.norm_extra;
+    a.diff_extra_first = warm ? 2.0 * sdev : 0.0;
+    a.warm = warm ? 1 : 0;
+    a.max_iter = max_iter;
+    a.tol = tol;
+    // device set-up of the intermediates, all inside the scratch array
+    noalloc_moduli_kernel<<<256, 256, 0, st>>>(E_dev, nu_dev, (int)N, D, plane_stress != 0, lam, mu);
+    for (int i = 0; i < D; ++i) {
+        auto* t64 = reinterpret_cast<cplx<double>*>(base + o_tw64[i]);
+        auto* t32 = reinterpret_cast<cplx<float>*>(base + o_tw32[i]);
+        noalloc_twiddle_kernel<<<(dims[i] + 255) / 256, 256, 0, st>>>(dims[i], t64, t32);
+        a.ax[i].tw64 = t64;
+        a.ax[i].tw32 = t32;
+    }
+    if (warm) {
+        if (D == 2) split_tensor_kernel<2><<<256, 256, 0, st>>>(eps_dev, (int)N, eps_s);
+        else split_tensor_kernel<3><<<256, 256, 0, st>>>(eps_dev, (int)N, eps_s);
+    }
+    if (epsp_s) {
+        if (D == 2) split_tensor_kernel<2><<<256, 256, 0, st>>>(eps_plastic_dev, (int)N, epsp_s);
+        else split_tensor_kernel<3><<<256, 256, 0, st>>>(eps_plastic_dev, (int)N, epsp_s);
+    }
+    // barrier words and the error word must start at zero on every call
+    e = cudaMemsetAsync(base + o_bar, 0, 4 * sizeof(unsigned), st);
+    if (e != cudaSuccess) return noalloc_fail(MGK_CUDA_ERROR, cudaGetErrorString(e));
+    a.eps_s = eps_s;
+    a.epsp_s = epsp_s;
+    a.lam = lam;
+    a.mu = mu;
+    a.spec = base + o_spec;
+    a.partials = reinterpret_cast<double*>(base + o_part);
+    a.result = reinterpret_cast<LsResult*>(base + o_res);
+    a.bar = reinterpret_cast<unsigned*>(base + o_bar);
+    a.err = a.bar + 2;
+    void* params[] = {&a};
+    e = cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(256), params, smem, st);
+    if (e != cudaSuccess) return noalloc_fail(MGK_CUDA_ERROR, std::string("LS launch: ") + cudaGetErrorString(e));
+    if (D == 2) full_tensor_kernel<2><<<256, 256, 0, st>>>(eps_s, nullptr, lam, mu, wbar[0], wbar[1], wbar[2], (int)N, 0, eps_dev);
+    else full_tensor_kernel<3><<<256, 256, 0, st>>>(eps_s, nullptr, lam, mu, wbar[0], wbar[1], wbar[2], (int)N, 0, eps_dev);
+    if (sig_dev) {
+        if (D == 2) full_tensor_kernel<2><<<256, 256, 0, st>>>(eps_s, epsp_s, lam, mu, wbar[0], wbar[1], wbar[2], (int)N, 1, sig_dev);
+        else full_tensor_kernel<3><<<256, 256, 0, st>>>(eps_s, epsp_s, lam, mu, wbar[0], wbar[1], wbar[2], (int)N, 1, sig_dev);
+    }
+    LsResult res{};
+    unsigned err_word = 0;
+    e = cudaMemcpyAsync(&res, a.result, sizeof(LsResult), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err_word, a.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_fail(MGK_CUDA_ERROR, cudaGetErrorString(e));
+    if (err_word) return noalloc_fail(MGK_DEVICE_TIMEOUT, "device wait timed out in the LS solver");
+    if (macro_out) {
+        const double invN = 1.0 / (double)N, mean2mu = sum_two_mu * invN;
+        for (int i = 0; i < D; ++i)
+            for (int j = 0; j < D; ++j) {
+                const int c = sym_idx(D, i, j);
+                const double w = (i == j) ? 0.0 : wbar[(D == 2) ? 0 : (i + j - 1)];
+                const double sgn = (i < j) ? 1.0 : -1.0;
+                macro_out[i * D + j] = res.sum_s[c] * invN + sgn * w;
+                macro_out[DD + i * D + j] = res.sum_sig[c] * invN + sgn * w * mean2mu;
+            }
+    }
+    if (iters_out) *iters_out = res.iters;
+    if (res.iters >= max_iter && max_iter > 0 && !(res.diff < tol)) return MGK_LS_NOT_CONVERGED;
+    return MGK_OK;
+}
