@@ -47,7 +47,8 @@ MGK_API int mgk_device_count(void);
  * callers do before them (green_operator_2d/3d, :70-119 / :344-396; the
  * operator is evaluated on the fly, so there is no Gamma argument).
  * mgk_ls_create: dim 2 or 3; nz ignored for dim 2; plane_stress selects
- * compute_lame_2d's plane-stress branch (dim 2 only); E, nu: N host values. */
+ * compute_lame_2d's plane-stress branch (dim 2 only); E, nu: N host values.
+ * Axis lengths must factor into 2, 3, 5 and 7 (MGK_BAD_SHAPE otherwise). */
 typedef struct mgk_ls mgk_ls;
 MGK_API mgk_status mgk_ls_create(mgk_ls** out, int dim, int nx, int ny, int nz, int plane_stress, double pixel, const double* E,
                          const double* nu);

@@ -1,6 +1,9 @@
 // Batched in-CTA FFTs for the Lippmann-Schwinger passes.
 //
-// Lines of length n sit contiguously in shared memory (line l at buf + l*n).
+// Lines of length n sit in shared memory at a padded stride: element e of line
+// l is at buf[l * pad_len(n) + pad_idx(e)], one spare slot after every 8
+// elements, so the radix-strided 16-byte accesses of a stage spread over the
+// banks.
 // Each stage is a mixed-radix Stockham step (out-of-place between two shared
 // buffers, natural-order output): stage s with radix R and Ns = product of the
 // radices before it maps input element j + r*(n/R) through the twiddle
@@ -93,20 +96,24 @@ MGK_DEV void small_dft(cplx<T>* v, int sign, const cplx<T>* tw, int n) {
     }
 }
 
+MGK_DEV int pad_idx(int e) { return e + (e >> 3); }
+MGK_DEV int pad_len(int n) { return n + (n >> 3) + 1; }
+
 template <typename T, int R>
 MGK_DEV void fft_stage(const cplx<T>* __restrict__ in, cplx<T>* __restrict__ out, int nlines, int n, int Ns,
                        const cplx<T>* __restrict__ tw, int sign) {
     const int m = n / R;
     const int tstep = n / (Ns * R);
     const int total = nlines * m;
+    const int ls = pad_len(n);
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
         const int l = idx / m, j = idx - l * m;
-        const cplx<T>* src = in + l * n;
-        cplx<T>* dst = out + l * n;
+        const cplx<T>* src = in + l * ls;
+        cplx<T>* dst = out + l * ls;
         const int k = j % Ns;
         cplx<T> v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = src[j + r * m];
+        for (int r = 0; r < R; ++r) v[r] = src[pad_idx(j + r * m)];
         if (Ns > 1) {
 #pragma unroll
             for (int r = 1; r < R; ++r) {
@@ -118,7 +125,7 @@ MGK_DEV void fft_stage(const cplx<T>* __restrict__ in, cplx<T>* __restrict__ out
         small_dft<T, R>(v, sign, tw, n);
         const int d = (j / Ns) * Ns * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) dst[d + r * Ns] = v[r];
+        for (int r = 0; r < R; ++r) dst[pad_idx(d + r * Ns)] = v[r];
     }
 }
 
@@ -137,8 +144,6 @@ MGK_DEV cplx<T>* fft_lines(cplx<T>* a, cplx<T>* b, int nlines, const FftAxis& ax
             case 5: fft_stage<T, 5>(a, b, nlines, ax.n, Ns, tw, sign); break;
             case 7: fft_stage<T, 7>(a, b, nlines, ax.n, Ns, tw, sign); break;
             case 8: fft_stage<T, 8>(a, b, nlines, ax.n, Ns, tw, sign); break;
-            case 11: fft_stage<T, 11>(a, b, nlines, ax.n, Ns, tw, sign); break;
-            case 13: fft_stage<T, 13>(a, b, nlines, ax.n, Ns, tw, sign); break;
             default: break;  // host planner only emits the radices above
         }
         Ns *= R;

@@ -102,7 +102,8 @@ MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, dou
 #pragma unroll
     for (int c = 0; c < S; ++c) w += (c < D ? 1.0 : 2.0) * sg[c] * cs[c];
     const double wv = 0.5 * p.volume * (w / 1e9) * 6.241509;
-    return s.Q0[i] * exp(-geff) - wv;
+    // exp(-0) is exactly 1: skip the exponential for unsoftened voxels
+    return (geff == 0.0 ? s.Q0[i] : s.Q0[i] * exp(-geff)) - wv;
 }
 
 MGK_DEV double rate_of(const KmcPhys& p, double q, bool* inc) {
@@ -127,19 +128,21 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(KmcDevState s, Kmc
     const long base = (long)blockIdx.x * blockDim.x * items;
     dd acc = {0.0, 0.0};
     int unst = 0, last = -1;
+#pragma unroll 4
     for (int j = 0; j < items; ++j) {
         const long i = base + (long)j * blockDim.x + threadIdx.x;
-        if (i >= s.NM) break;
-        const int v = (int)(i / s.M);
-        const double q = mode_Q<D, C>(s, p, v, i, time);
-        s.Q[i] = q;
-        bool inc;
-        const double r = rate_of(p, q, &inc);
-        if (inc) {
-            last = (int)i;
-            acc = dd_add_d(acc, r);
+        if (i < s.NM) {
+            const int v = (int)(i / s.M);
+            const double q = mode_Q<D, C>(s, p, v, i, time);
+            s.Q[i] = q;
+            bool inc;
+            const double r = rate_of(p, q, &inc);
+            if (inc) {
+                last = (int)i;
+                acc = dd_add_d(acc, r);
+            }
+            if (q < p.threshold) ++unst;
         }
-        if (q < p.threshold) ++unst;
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     acc = warp_dd_sum(acc);
@@ -337,9 +340,11 @@ __global__ void __launch_bounds__(512) select_flip_kernel(KmcDevState s, KmcPhys
     for (int b = b0; b < b1; ++b) mine = dd_add(mine, blk[b]);
     dd tot;
     dd run = block_excl_scan(mine, sh, &tot);
+    int my_blk = -1;
     for (int b = b0; b < b1; ++b) {
         dd nx = dd_add(run, blk[b]);
         if (dd_ge(nx, target)) {
+            my_blk = b;
             atomicMin(&s_blk, b);
             break;
         }
@@ -348,12 +353,8 @@ __global__ void __launch_bounds__(512) select_flip_kernel(KmcDevState s, KmcPhys
     __syncthreads();
     const int cb = s_blk;
     if (cb != 0x7fffffff) {
-        // prefix before block cb, recomputed in fixed order by thread 0
-        if (threadIdx.x == 0) {
-            dd pre = {0.0, 0.0};
-            for (int b = 0; b < cb; ++b) pre = dd_add(pre, blk[b]);
-            s_before = pre;
-        }
+        // prefix before block cb: the exclusive prefix of the thread that found it
+        if (my_blk == cb) s_before = run;
         __syncthreads();
         // 2. inside block cb: contiguous runs per thread, mode order
         const long m0 = (long)cb * kSweepThreads * items;

@@ -134,6 +134,7 @@ MGK_DEV void row_pass(const LsArgs& a, cplx<T>* buf0, cplx<T>* buf1, double* par
     const long cs = (long)a.nrows * nh;
     const int nchunks = (a.nrows + a.rpb - 1) / a.rpb;
     const FftAxis& ax = a.ax[D - 1];
+    const int lsn = pad_len(n);
     for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
         const int row0 = ch * a.rpb;
         const int rows = min(a.rpb, a.nrows - row0);
@@ -154,7 +155,7 @@ MGK_DEV void row_pass(const LsArgs& a, cplx<T>* buf0, cplx<T>* buf1, double* par
                     A = cconj(A);
                     B = cconj(B);
                 }
-                z[idx] = {A.x - B.y, A.y + B.x};
+                z[p * lsn + pad_idx(k)] = {A.x - B.y, A.y + B.x};
             }
             __syncthreads();
             z = fft_lines<T>(buf0, buf1, P, ax, +1);
@@ -170,7 +171,7 @@ MGK_DEV void row_pass(const LsArgs& a, cplx<T>* buf0, cplx<T>* buf1, double* par
                 const double so = a.eps_s[(long)c * N + v];
                 if (MODE == 1) {
                     const int l = r * S + c;
-                    const cplx<T> zz = z[(l >> 1) * n + y];
+                    const cplx<T> zz = z[(l >> 1) * lsn + pad_idx(y)];
                     const double et = (double)((l & 1) ? zz.y : zz.x) * a.inv_n;
                     sn[c] = a.ebar_s[c] + et;
                     const double wc = c < D ? 1.0 : 2.0;
@@ -199,7 +200,7 @@ MGK_DEV void row_pass(const LsArgs& a, cplx<T>* buf0, cplx<T>* buf1, double* par
                 part[2 + c] += sn[c];
                 part[2 + S + c] += sig;
                 const int l = r * S + c;
-                cplx<T>* cell = &z[(l >> 1) * n + y];
+                cplx<T>* cell = &z[(l >> 1) * lsn + pad_idx(y)];
                 if (l & 1) {
                     cell->y = (T)(sig - sig0);
                 } else {
@@ -213,8 +214,8 @@ MGK_DEV void row_pass(const LsArgs& a, cplx<T>* buf0, cplx<T>* buf1, double* par
         __syncthreads();
         for (int idx = threadIdx.x; idx < P * nh; idx += blockDim.x) {
             const int p = idx / nh, k = idx - p * nh;
-            const cplx<T> zk = Z[p * n + k];
-            const cplx<T> zm = cconj(Z[p * n + (k == 0 ? 0 : n - k)]);
+            const cplx<T> zk = Z[p * lsn + pad_idx(k)];
+            const cplx<T> zm = cconj(Z[p * lsn + pad_idx(k == 0 ? 0 : n - k)]);
             const int la = 2 * p, lb = 2 * p + 1;
             const cplx<T> A = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y + zm.y)};
             spec[(la % S) * cs + (long)(row0 + la / S) * nh + k] = A;
@@ -251,6 +252,7 @@ MGK_DEV void strided_pass(const LsArgs& a, int axis, cplx<T>* buf0, cplx<T>* buf
     const int items = no * ntk;
     const int nl = S * tk;
     const FftAxis& fx = a.ax[axis];
+    const int lsn = pad_len(n);
     for (int it = blockIdx.x; it < items; it += gridDim.x) {
         const int o = it / ntk;
         const int k0 = (it - o * ntk) * tk;
@@ -260,7 +262,7 @@ MGK_DEV void strided_pass(const LsArgs& a, int axis, cplx<T>* buf0, cplx<T>* buf
             const int t = idx % tk;
             const int i = (idx / tk) % n;
             const int c = idx / (tk * n);
-            buf0[(c * tk + t) * n + i] = (t < tku) ? spec[c * cs + base + t + i * st] : cplx<T>{T(0), T(0)};
+            buf0[(c * tk + t) * lsn + pad_idx(i)] = (t < tku) ? spec[c * cs + base + t + i * st] : cplx<T>{T(0), T(0)};
         }
         __syncthreads();
         cplx<T>* Z = fft_lines<T>(buf0, buf1, nl, fx, KIND == 1 ? +1 : -1);
@@ -285,10 +287,10 @@ MGK_DEV void strided_pass(const LsArgs& a, int axis, cplx<T>* buf0, cplx<T>* buf
                 }
                 cplx<T> tv[S];
 #pragma unroll
-                for (int c = 0; c < S; ++c) tv[c] = Z[(c * tk + t) * n + kx];
+                for (int c = 0; c < S; ++c) tv[c] = Z[(c * tk + t) * lsn + pad_idx(kx)];
                 green_apply<D, T>(q, nyq, tv, a.inv2mu0, a.bcoef);
 #pragma unroll
-                for (int c = 0; c < S; ++c) Z[(c * tk + t) * n + kx] = tv[c];
+                for (int c = 0; c < S; ++c) Z[(c * tk + t) * lsn + pad_idx(kx)] = tv[c];
             }
             __syncthreads();
             cplx<T>* other = (Z == buf0) ? buf1 : buf0;
@@ -299,7 +301,7 @@ MGK_DEV void strided_pass(const LsArgs& a, int axis, cplx<T>* buf0, cplx<T>* buf
             const int t = idx % tk;
             const int i = (idx / tk) % n;
             const int c = idx / (tk * n);
-            if (t < tku) spec[c * cs + base + t + i * st] = Z[(c * tk + t) * n + i];
+            if (t < tku) spec[c * cs + base + t + i * st] = Z[(c * tk + t) * lsn + pad_idx(i)];
         }
         __syncthreads();
     }
@@ -313,18 +315,29 @@ MGK_DEV void publish_partials(const LsArgs& a, double* part, double* red) {
 }
 
 // Every CTA reduces all partials in the same fixed order -> identical values.
+// 256 threads: thread t sums value (t & 15) over blocks (t >> 4), (t >> 4) + 16, ...;
+// then the 16 group sums are added in group order.
 template <int NP>
 MGK_DEV void gather_partials(const LsArgs& a, double* out /* shared, NP */) {
+    __shared__ double grp[256];
+    const int k = threadIdx.x & 15, g = threadIdx.x >> 4;
+    double s = 0.0;
+    if (k < NP) {
+#pragma unroll 4
+        for (unsigned b = g; b < gridDim.x; b += 16) s += __ldcg(&a.partials[b * kMaxPartials + k]);
+    }
+    grp[threadIdx.x] = s;
+    __syncthreads();
     if (threadIdx.x < NP) {
-        double s = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(&a.partials[b * kMaxPartials + threadIdx.x]);
-        out[threadIdx.x] = s;
+        double t = 0.0;
+        for (int gg = 0; gg < 16; ++gg) t += grp[gg * 16 + threadIdx.x];
+        out[threadIdx.x] = t;
     }
     __syncthreads();
 }
 
 template <int D, typename T>
-__global__ void __launch_bounds__(256) ls_kernel(const __grid_constant__ LsArgs a) {
+__global__ void __launch_bounds__(256, 2) ls_kernel(const __grid_constant__ LsArgs a) {
     constexpr int S = D == 2 ? 3 : 6;
     constexpr int NP = 2 + 2 * S;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -454,13 +467,16 @@ __global__ void split_tensor_kernel(const double* __restrict__ full, int N, doub
 }  // namespace
 
 // ---------------------------------------------------------------- host side
+// shared-memory line length of a length-n transform (pad_len in fft.cuh)
+static size_t padded_len(int n) { return (size_t)n + (size_t)(n >> 3) + 1; }
+
 bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned) {
     std::memset(ax, 0, sizeof(*ax));
     ax->n = n;
     int m = n, k = 0;
     while (m % 8 == 0 && m >= 64 && k < kMaxStages) { ax->radix[k++] = 8; m /= 8; }
     while (m % 4 == 0 && k < kMaxStages) { ax->radix[k++] = 4; m /= 4; }
-    static const int primes[] = {2, 3, 5, 7, 11, 13};
+    static const int primes[] = {2, 3, 5, 7};
     for (int p : primes)
         while (m % p == 0 && k < kMaxStages) { ax->radix[k++] = p; m /= p; }
     if (m != 1) return false;
@@ -541,7 +557,7 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     a.bcoef = (lam0_ + mu0_) / (mu0_ * (lam0_ + 2.0 * mu0_));
     a.pixel = pixel;
     for (int i = 0; i < D; ++i)
-        if (!plan_axis(dims_[i], &a.ax[i], &tw_bufs_)) throw std::invalid_argument("unsupported FFT length (prime factor > 13)");
+        if (!plan_axis(dims_[i], &a.ax[i], &tw_bufs_)) throw std::invalid_argument("unsupported FFT length (prime factor > 7)");
     // decomposition
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -554,9 +570,9 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     const int col_items = ((D == 2) ? 1 : std::min(dims_[0], dims_[1])) * ((nh + a.tk - 1) / a.tk);
     // shared memory: two buffers of the largest pass
     const size_t elem = sizeof(cplx<double>);
-    const size_t row_b = (size_t)((a.rpb * S_ + 1) / 2) * nr * elem;
+    const size_t row_b = (size_t)((a.rpb * S_ + 1) / 2) * padded_len(nr) * elem;
     size_t col_b = 0;
-    for (int ax = 0; ax < D - 1; ++ax) col_b = std::max(col_b, (size_t)S_ * a.tk * dims_[ax] * elem);
+    for (int ax = 0; ax < D - 1; ++ax) col_b = std::max(col_b, (size_t)S_ * a.tk * padded_len(dims_[ax]) * elem);
     const size_t half_b = (std::max(row_b, col_b) + 127) / 128 * 128;
     smem_ = 2 * half_b;
     a.smem_half = (int)half_b;
@@ -820,7 +836,7 @@ bool noalloc_radices(int n, FftAxis* ax) {
     int m = n, k = 0;
     while (m % 8 == 0 && m >= 64 && k < kMaxStages) { ax->radix[k++] = 8; m /= 8; }
     while (m % 4 == 0 && k < kMaxStages) { ax->radix[k++] = 4; m /= 4; }
-    static const int primes[] = {2, 3, 5, 7, 11, 13};
+    static const int primes[] = {2, 3, 5, 7};
     for (int p : primes)
         while (m % p == 0 && k < kMaxStages) { ax->radix[k++] = p; m /= p; }
     ax->nst = k;
@@ -862,7 +878,7 @@ mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stres
     a.nr = nr;
     a.nh = nh;
     for (int i = 0; i < D; ++i)
-        if (!noalloc_radices(dims[i], &a.ax[i])) return noalloc_fail(MGK_BAD_SHAPE, "unsupported FFT length (prime factor > 13)");
+        if (!noalloc_radices(dims[i], &a.ax[i])) return noalloc_fail(MGK_BAD_SHAPE, "unsupported FFT length (prime factor > 7)");
     // decomposition: the same rules as LsSolver
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -874,9 +890,9 @@ mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stres
     const long row_items = (nrows + a.rpb - 1) / a.rpb;
     const long col_items = (long)((D == 2) ? 1 : std::min(dims[0], dims[1])) * ((nh + a.tk - 1) / a.tk);
     const size_t elem = sizeof(cplx<double>);
-    const size_t row_b = (size_t)((a.rpb * S + 1) / 2) * nr * elem;
+    const size_t row_b = (size_t)((a.rpb * S + 1) / 2) * padded_len(nr) * elem;
     size_t col_b = 0;
-    for (int ax = 0; ax < D - 1; ++ax) col_b = std::max(col_b, (size_t)S * a.tk * dims[ax] * elem);
+    for (int ax = 0; ax < D - 1; ++ax) col_b = std::max(col_b, (size_t)S * a.tk * padded_len(dims[ax]) * elem);
     const size_t half_b = (std::max(row_b, col_b) + 127) / 128 * 128;
     const size_t smem = 2 * half_b;
     a.smem_half = (int)half_b;

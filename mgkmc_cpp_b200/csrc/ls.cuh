@@ -122,8 +122,8 @@ private:
     size_t smem_ = 0, bytes_ = 0;
 };
 
-// Plans the radix sequence of a length-n transform (radix-4 first, then 2, 3,
-// 5, 7, 8, 11, 13).  Returns false for lengths with other prime factors.
+// Plans the radix sequence of a length-n transform (radix-8 while n >= 64,
+// radix-4, then 2, 3, 5, 7).  Returns false for lengths with other prime factors.
 bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned);
 
 }  // namespace mgk
