@@ -33,7 +33,8 @@ typedef enum {
     MGK_CUDA_ERROR = 5,
     MGK_BAD_ARG = 6,
     MGK_UNSUPPORTED = 7,      /* option not built (e.g. fast patching) */
-    MGK_TERMINATED = 8        /* KMC instability sequence limit (kmc_solver.hpp:925-929) */
+    MGK_TERMINATED = 8,       /* KMC instability sequence limit (kmc_solver.hpp:925-929) */
+    MGK_TIME_LIMIT = 9        /* a batched run reached its wall-time limit (mgk_batch_set_time_limit) */
 } mgk_status;
 
 /* Text of the last error on this thread. */
@@ -153,6 +154,36 @@ MGK_API mgk_status mgk_kmc_get_field(mgk_kmc* h, int field, double* dst, long lo
  * host synchronisations, kernel launches. */
 MGK_API mgk_status mgk_kmc_get_macro(mgk_kmc* h, double* out, int n);
 MGK_API void mgk_kmc_destroy(mgk_kmc* h);
+
+/* ---------------------------------------------------------------- batched, device-resident KMC
+ * No counterpart in the reference (single replica, single thread there).  n
+ * independent simulations, each constructed exactly like mgk_kmc_create, run
+ * together by one persistent GPU kernel: every replica's run_simulation
+ * control flow (sweep, selection, flip, LS solve, cascades, mixed-BC loop)
+ * executes on the device with no host round trip per event, each replica on
+ * its own group of CTAs.  The random stream is the reference's: each replica's
+ * std::mt19937 state continues on the device with the same distributions.
+ * mgk_batch_run advances every replica by up to max_events thermal events
+ * (<= 0: until its n_global_steps elastic steps are done); rp holds n entries
+ * (log and VTU fields are ignored: device-resident runs write no files);
+ * elapsed_ms gets the kernel's CUDA-event time.  mgk_batch_stats fills
+ * out[0..9] = {events, cascades, cascade flips, LS solves, LS iterations,
+ * elastic steps, selection fallbacks, smallest selection margin, terminated
+ * (1 instability sequence limit, 2 time limit), CTAs of the replica} and
+ * copies the flat mode index of each thermal event of the last run into sel
+ * (up to sel_cap; *sel_len gets the count).  A run stops every replica whose
+ * run call has lasted longer than the time limit (default 60 s, set with
+ * mgk_batch_set_time_limit) at its next decision and returns MGK_TIME_LIMIT;
+ * the state stays consistent and a later run continues from it. */
+typedef struct mgk_batch mgk_batch;
+MGK_API mgk_status mgk_batch_create(mgk_batch** out, int n, const mgk_kmc_params* params, const double* const* E,
+                                    const double* const* nu);
+MGK_API mgk_status mgk_batch_run(mgk_batch* h, const mgk_run_params* rp, long long max_events, double* elapsed_ms);
+MGK_API mgk_status mgk_batch_stats(mgk_batch* h, int replica, double* out, int* sel, long long sel_cap, long long* sel_len);
+MGK_API mgk_status mgk_batch_get_field(mgk_batch* h, int replica, int field, double* dst, long long* count);
+MGK_API mgk_status mgk_batch_get_macro(mgk_batch* h, int replica, double* out, int n);
+MGK_API mgk_status mgk_batch_set_time_limit(mgk_batch* h, double seconds);
+MGK_API void mgk_batch_destroy(mgk_batch* h);
 
 /* Measurement hooks (no counterpart in the reference, which only logs wall
  * time).  mgk_kmc_set_profiling(h, 1) clears the profile and records CUDA

@@ -27,7 +27,7 @@ from . import _lib
 from ._lib import MgkError
 
 __all__ = ["BarrierGenerator", "LsSolver", "spectral_solver_2d", "spectral_solver_3d", "KmcSimulation2D",
-           "KmcSimulation3D", "from_config", "MgkError"]
+           "KmcSimulation3D", "KmcBatch", "from_config", "MgkError"]
 
 _BAR = {"gaussian": 0, "rayleigh": 1, "modified_rayleigh": 2, "modified_rayleigh_with_exponential": 3}
 
@@ -321,3 +321,126 @@ def from_config(cfg, output_dir: Optional[str] = None):
         return KmcSimulation3D(cfg.nx, cfg.ny, cfg.nz, cfg.M, cfg.gamma0, cfg.E, cfg.nu,
                                use_3d_barriers=cfg.use_3d_barriers, **kw)
     return KmcSimulation2D(cfg.nx, cfg.ny, cfg.M, cfg.gamma0, cfg.E, cfg.nu, plane_mode=cfg.plane_mode, **kw)
+
+
+def kmc_params_from_config(cfg) -> "_lib.KmcParamsC":
+    """mgk_kmc_params for a SimConfig (the values main.cpp:278-317 passes)."""
+    b = cfg.barrier
+    if b.type not in _BAR:
+        raise ValueError("unknown barrier type %r" % b.type)
+    p = _lib.KmcParamsC()
+    p.dim, p.nx, p.ny, p.nz, p.M = cfg.dim, cfg.nx, cfg.ny, cfg.nz if cfg.dim == 3 else 1, cfg.M
+    p.plane_stress = 1 if cfg.plane_mode == "plane_stress" else 0
+    p.seed, p.gamma0, p.pixel = int(cfg.seed), float(cfg.gamma0), float(cfg.pixel)
+    p.barrier_type = _BAR[b.type]
+    p.bar_mean, p.bar_std, p.bar_min_cutoff, p.bar_max_cutoff = b.mean, b.std, b.min_cutoff, b.max_cutoff
+    p.bar_loc, p.bar_scale, p.bar_epsilon, p.bar_ratio = b.loc, b.scale, b.epsilon, b.ratio
+    p.directional = 1 if cfg.softening_scheme == "directional" else 0
+    p.softening_cap, p.jp, p.jt = cfg.softening_cap, cfg.jp, cfg.jt
+    p.neighbor_fraction, p.q_act_temp = cfg.neighbor_softening_fraction, cfg.q_act_temp
+    p.temperature, p.strain_rate, p.stability_threshold, p.nu0 = (cfg.temperature, cfg.strain_rate,
+                                                                   cfg.stability_threshold, cfg.nu0)
+    p.instability_kmc = 1 if cfg.instability_mode == "kmc" else 0
+    p.scale_rate_by_volume = int(bool(cfg.scale_rate_by_volume))
+    p.redraw_directions, p.redraw_barriers = int(bool(cfg.redraw_directions)), int(bool(cfg.redraw_barriers))
+    p.use_3d_barriers = int(bool(cfg.use_3d_barriers))
+    p.fast_patching, p.patch_radius, p.sync_interval = int(bool(cfg.fast_patching)), cfg.patch_radius, cfg.sync_interval
+    p.ls_tol, p.ls_max_iter = float(cfg.ls_tol), int(cfg.ls_max_iter)
+    return p
+
+
+def run_params_from_config(cfg, n_global_steps=None, max_cascade_batches=0) -> "_lib.RunParamsC":
+    rp = _lib.RunParamsC()
+    rp.n_global_steps = int(cfg.n_steps if n_global_steps is None else n_global_steps)
+    rp.step_size = float(cfg.step_size)
+    rp.comp_i, rp.comp_j = cfg.driving
+    tg = sorted(cfg.targets.items())
+    rp.n_targets = len(tg)
+    for k, ((i, j), v) in enumerate(tg):
+        rp.target_i[k], rp.target_j[k], rp.target_v[k] = i, j, v
+    rp.mixed_tol, rp.mixed_max_iter, rp.max_kmc_steps_pct = cfg.mixed_tol_pa, 50, cfg.max_kmc_steps_pct
+    rp.max_events = 0
+    rp.output_dir = None
+    rp.summary_filename = b"summary_log.txt"
+    rp.vtk_interval = b"none"
+    rp.vtk_elastic_only = 1
+    rp.max_cascade_batches = int(max_cascade_batches)
+    return rp
+
+
+class KmcBatch:
+    """Replicas advanced together by one device-resident kernel (mgk_batch_*):
+    no host round trip per event; the reference's random stream continued on
+    the device.  ``configs`` is a list of SimConfig."""
+
+    def __init__(self, configs):
+        L = _lib.lib()
+        _lib.require_device()
+        self.cfgs = list(configs)
+        n = len(self.cfgs)
+        self._params = (_lib.KmcParamsC * n)(*[kmc_params_from_config(c) for c in self.cfgs])
+        self._E = [np.ascontiguousarray(c.E, dtype=np.float64).reshape(-1) for c in self.cfgs]
+        self._nu = [np.ascontiguousarray(c.nu, dtype=np.float64).reshape(-1) for c in self.cfgs]
+        dp = _lib.C.POINTER(_lib.C.c_double)
+        Ep = (dp * n)(*[_lib.dptr(a) for a in self._E])
+        np_ = (dp * n)(*[_lib.dptr(a) for a in self._nu])
+        h = _lib.C.c_void_p()
+        _lib.check(L.mgk_batch_create(_lib.C.byref(h), n, self._params, Ep, np_))
+        self._h = h
+
+    def set_time_limit(self, seconds: float):
+        """Wall-time bound of one run call (default 60 s)."""
+        _lib.check(_lib.lib().mgk_batch_set_time_limit(self._h, float(seconds)))
+
+    def run(self, max_events: int, n_global_steps=10 ** 6, max_cascade_batches=0) -> float:
+        """Advance every replica by up to max_events thermal events; returns
+        the kernel time in milliseconds.  A run that reaches the time limit
+        returns normally with ``self.time_limited`` set."""
+        n = len(self.cfgs)
+        rps = (_lib.RunParamsC * n)(*[run_params_from_config(c, n_global_steps, max_cascade_batches) for c in self.cfgs])
+        ms = np.zeros(1)
+        st = _lib.lib().mgk_batch_run(self._h, rps, int(max_events), _lib.dptr(ms))
+        self.time_limited = st == 9
+        if st not in (0, 9):
+            _lib.check(st)
+        return float(ms[0])
+
+    def stats(self, r: int) -> dict:
+        out = np.zeros(10)
+        cap = 1 << 16
+        sel = (_lib.C.c_int * cap)()
+        ln = _lib.C.c_longlong(0)
+        _lib.check(_lib.lib().mgk_batch_stats(self._h, r, _lib.dptr(out), sel, cap, _lib.C.byref(ln)))
+        keys = ["events", "cascades", "cascade_flips", "ls_solves", "ls_iters", "elastic_steps", "fallbacks",
+                "min_margin", "terminated", "ctas"]
+        d = {k: float(v) for k, v in zip(keys, out)}
+        d["selected"] = np.array(sel[:min(ln.value, cap)], dtype=np.int64)
+        return d
+
+    def field(self, r: int, name: str) -> np.ndarray:
+        f = _FIELDS[name]
+        n = _lib.C.c_longlong(0)
+        _lib.check(_lib.lib().mgk_batch_get_field(self._h, r, f, None, _lib.C.byref(n)))
+        out = np.zeros(n.value)
+        _lib.check(_lib.lib().mgk_batch_get_field(self._h, r, f, _lib.dptr(out), None))
+        D = self.cfgs[r].dim
+        if name in ("eps_field", "sig_field", "eps_plastic", "prev_strain_dir", "catalog"):
+            return out.reshape(-1, D, D)
+        return out
+
+    def macro(self, r: int) -> np.ndarray:
+        D = self.cfgs[r].dim
+        out = np.zeros(2 * D * D + 10)
+        _lib.check(_lib.lib().mgk_batch_get_macro(self._h, r, _lib.dptr(out), out.size))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().mgk_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

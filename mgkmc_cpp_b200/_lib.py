@@ -12,11 +12,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmgkmc_b200.so")
 
 STATUS = {0: "MGK_OK", 1: "MGK_LS_NOT_CONVERGED", 2: "MGK_BAD_SHAPE", 3: "MGK_OOM", 4: "MGK_DEVICE_TIMEOUT",
-          5: "MGK_CUDA_ERROR", 6: "MGK_BAD_ARG", 7: "MGK_UNSUPPORTED", 8: "MGK_TERMINATED"}
+          5: "MGK_CUDA_ERROR", 6: "MGK_BAD_ARG", 7: "MGK_UNSUPPORTED", 8: "MGK_TERMINATED",
+          9: "MGK_TIME_LIMIT"}
 
 EXPORTS = ["mgk_last_error", "mgk_version", "mgk_device_count", "mgk_ls_create", "mgk_ls_solve", "mgk_ls_destroy",
            "mgk_kmc_create", "mgk_kmc_run", "mgk_kmc_elastic_run", "mgk_kmc_get_field", "mgk_kmc_get_macro",
-           "mgk_kmc_destroy", "mgk_kmc_set_profiling", "mgk_kmc_get_profile"]
+           "mgk_kmc_destroy", "mgk_kmc_set_profiling", "mgk_kmc_get_profile", "mgk_batch_create", "mgk_batch_run",
+           "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro", "mgk_batch_set_time_limit",
+           "mgk_batch_destroy"]
 
 
 class MgkError(RuntimeError):
@@ -77,10 +80,20 @@ def lib():
     L.mgk_kmc_get_macro.argtypes = [vp, dp, C.c_int]
     L.mgk_kmc_set_profiling.argtypes = [vp, C.c_int]
     L.mgk_kmc_get_profile.argtypes = [vp, dp, dp, C.c_longlong]
+    L.mgk_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(KmcParamsC), C.POINTER(dp), C.POINTER(dp)]
+    L.mgk_batch_run.argtypes = [vp, C.POINTER(RunParamsC), C.c_longlong, dp]
+    L.mgk_batch_stats.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_int), C.c_longlong, C.POINTER(C.c_longlong)]
+    L.mgk_batch_get_field.argtypes = [vp, C.c_int, C.c_int, dp, C.POINTER(C.c_longlong)]
+    L.mgk_batch_get_macro.argtypes = [vp, C.c_int, dp, C.c_int]
+    L.mgk_batch_set_time_limit.argtypes = [vp, C.c_double]
+    L.mgk_batch_destroy.argtypes = [vp]
+    L.mgk_batch_destroy.restype = None
     L.mgk_kmc_destroy.argtypes = [vp]
     L.mgk_kmc_destroy.restype = None
     for fn in ("mgk_ls_create", "mgk_ls_solve", "mgk_kmc_create", "mgk_kmc_run", "mgk_kmc_elastic_run",
-               "mgk_kmc_get_field", "mgk_kmc_get_macro", "mgk_kmc_set_profiling", "mgk_kmc_get_profile"):
+               "mgk_kmc_get_field", "mgk_kmc_get_macro", "mgk_kmc_set_profiling", "mgk_kmc_get_profile",
+               "mgk_batch_create", "mgk_batch_run", "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro",
+               "mgk_batch_set_time_limit"):
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L

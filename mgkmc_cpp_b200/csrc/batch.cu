@@ -1,0 +1,767 @@
+// Device-resident, batched KMC: many replicas advance inside one persistent
+// cooperative kernel, each replica on its own group of CTAs with its own
+// bounded group barrier, and no host round trip per event.
+//
+// Per replica the kernel runs the control flow of run_simulation
+// (kmc_solver.hpp:721-1037 / :1735-2062) on the device:
+//   sweep (update_barriers + rates, every CTA of the group over its chunk of
+//   modes) -> decision on the group's first CTA (total rate, u1 -> t_wait,
+//   event / end of interval / cascade; u2 -> target; selection over the chunk
+//   sums and then inside one chunk; flip with apply_flip_soa_* and the catalog
+//   and barrier redraw) -> warm-started LS solve by the whole group ->
+//   repeat; at the end of an interval the mixed-BC loop (:955-987); unstable
+//   modes run the cascade batches (:464-564).
+// Random numbers: the replica's std::mt19937 state after its host-side
+// initial draws is handed to the device and continued by one thread with the
+// reference's distributions (mt_device.cuh), so the draws follow the
+// reference's stream; only device log/exp may differ from glibc by an ulp.
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <sstream>
+#include <stdexcept>
+
+#include "batch.cuh"
+#include "kmc_device.cuh"
+#include "ls_device.cuh"
+#include "mt_device.cuh"
+
+namespace mgk {
+
+enum : int { ACT_EVENT = 1, ACT_CASCADE = 2, ACT_END = 3, ACT_STOP = 4 };
+
+MGK_DEV unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct BatchCtl {
+    double time, remaining, dt_step, strain_rate;
+    double eps_macro[9], sig_macro[9];
+    double w[3];
+    double sum_two_mu, Ea, na, mixed_tol, ls_tol;
+    double tv[9];
+    double min_margin;
+    int tflat[9], tdiag[9];
+    int n_targets, mixed_max_iter, ci, ls_max_iter;
+    int n_global_steps, elastic_done;
+    int seq_instab, max_seq;
+    int need_initial_solve;
+    int action, done, status;  // status: 0 ok, 1 instability limit reached, 2 time limit reached
+    int cascade_active, cascade_batches, mixed_it, ccount;
+    long long cascade_limit;
+    long long max_events, events_done;
+    long long events_total, cascades, cascade_flips, ls_solves, ls_iters, elastic_steps, fallbacks;
+    int sel_log_len, sel_log_cap;
+    unsigned long long t_start_ns, limit_ns;  // device clock at the first decision; 0: unset
+};
+
+struct BatchRep {
+    KmcDevState s;
+    KmcPhys p;
+    LsArgs ls;
+    rng::Barrier bg;
+    double gamma0;
+    int redraw_dir, redraw_bar, C, pad0;
+    int ncta;
+    unsigned* bar;  // {arrivals, generation, error, spare}
+    dd* chunk_sum;
+    int* chunk_unst;
+    int* chunk_last;
+    double* ckeys;
+    int* cmodes;
+    int ccap;
+    rng::Mt* mt;
+    BatchCtl* ctl;
+    int* sel_log;
+};
+
+namespace {
+
+using namespace kmcdev;
+
+MGK_DEV int vld(const int* p) { return *(const volatile int*)p; }
+
+// eps_macro / sig_macro of the last solve (as LsSolver::macro)
+template <int D>
+MGK_DEV void macro_from_result(const LsResult* r, BatchCtl* c, const double* w, int N) {
+    const double invN = 1.0 / (double)N, mean2mu = c->sum_two_mu * invN;
+    for (int i = 0; i < D; ++i)
+        for (int j = 0; j < D; ++j) {
+            const int k = lsdev::sym_idx(D, i, j);
+            const double ww = (i == j) ? 0.0 : w[(D == 2) ? 0 : (i + j - 1)];
+            const double sgn = (i < j) ? 1.0 : -1.0;
+            c->eps_macro[i * D + j] = r->sum_s[k] * invN + sgn * ww;
+            c->sig_macro[i * D + j] = r->sum_sig[k] * invN + sgn * ww * mean2mu;
+        }
+}
+
+// warm-started LS solve with eps_bar = eps_macro (elastic_run) by the group
+template <int D>
+MGK_DEV bool group_solve(BatchRep& R, int rank, const GridBar& gb, unsigned char* smem, LsArgs* sls) {
+    BatchCtl* c = R.ctl;
+    if (threadIdx.x == 0) {
+        *sls = R.ls;
+        double wbar[3] = {0, 0, 0};
+        const double* eb = c->eps_macro;
+        for (int i = 0; i < D; ++i)
+            for (int j = i; j < D; ++j) {
+                const int k = lsdev::sym_idx(D, i, j);
+                sls->ebar_s[k] = (i == j) ? eb[i * D + i] : 0.5 * (eb[i * D + j] + eb[j * D + i]);
+                if (i != j) wbar[(D == 2) ? 0 : (i + j - 1)] = 0.5 * (eb[i * D + j] - eb[j * D + i]);
+            }
+        double sw2 = 0.0;
+        for (int k = 0; k < (D == 2 ? 1 : 3); ++k) sw2 += wbar[k] * wbar[k];
+        sls->norm_extra = 2.0 * (double)sls->N * sw2;
+        sls->norm_extra_first = sls->norm_extra;  // the field's antisymmetric part is uniform
+        sls->diff_extra_first = 0.0;
+        sls->warm = 1;
+        sls->max_iter = c->ls_max_iter;
+        sls->tol = c->ls_tol;
+        sls->epsp_s = R.s.epsp_s;
+        if (rank == 0)
+            for (int k = 0; k < 3; ++k) c->w[k] = wbar[k];
+    }
+    __syncthreads();
+    if (!lsdev::ls_solve_group<D, double>(*sls, rank, R.ncta, gb, smem)) return false;
+    if (rank == 0 && threadIdx.x == 0) {
+        macro_from_result<D>(sls->result, c, c->w, R.s.N);
+        c->ls_solves++;
+        c->ls_iters += sls->result->iters;
+    }
+    return true;
+}
+
+template <int D, int C>
+MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
+    __shared__ dd sd[8];
+    __shared__ int si[8], sl[8];
+    const long NM = R.s.NM;
+    const long m0 = NM * rank / R.ncta, m1 = NM * (rank + 1) / R.ncta;
+    dd acc = {0.0, 0.0};
+    int unst = 0, last = -1;
+    for (long i = m0 + threadIdx.x; i < m1; i += blockDim.x) {
+        const int v = (int)(i / R.s.M);
+        const double q = mode_Q<D, C>(R.s, R.p, v, i, time);
+        R.s.Q[i] = q;
+        bool inc;
+        const double r = rate_of(R.p, q, &inc);
+        if (inc) {
+            last = (int)i;
+            acc = dd_add_d(acc, r);
+        }
+        if (q < R.p.threshold) ++unst;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    acc = warp_dd_sum(acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unst += __shfl_down_sync(0xffffffffu, unst, o);
+        last = max(last, __shfl_down_sync(0xffffffffu, last, o));
+    }
+    if (lane == 0) {
+        sd[wid] = acc;
+        si[wid] = unst;
+        sl[wid] = last;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        dd a = {0.0, 0.0};
+        int u = 0, l = -1;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a = dd_add(a, sd[w]);
+            u += si[w];
+            l = max(l, sl[w]);
+        }
+        R.chunk_sum[rank] = a;
+        R.chunk_unst[rank] = u;
+        R.chunk_last[rank] = l;
+    }
+    __syncthreads();
+}
+
+// Redraw after a flip of mode k (kmc_solver.hpp:839-864 / :1854-1875) with the
+// device stream; one thread.
+template <int C>
+MGK_DEV void redraw_dev(BatchRep& R, rng::Mt* mt, long k) {
+    const long v = k / R.s.M;
+    if (R.redraw_dir || R.redraw_bar) {
+        for (int mm = 0; mm < R.s.M; ++mm) {
+            const long ci = v * R.s.M + mm;
+            if (R.redraw_dir) rng::mode<C>(mt, R.gamma0, R.s.cat + ci * C);
+            if (R.redraw_bar) R.s.Q0[ci] = rng::barrier(R.bg, mt);
+        }
+    } else {
+        rng::mode<C>(mt, R.gamma0, R.s.cat + k * C);
+        R.s.Q0[k] = rng::barrier(R.bg, mt);
+    }
+}
+
+// First CTA of the group: decide the next action from the sweep; for an event
+// also select the mode and flip it.  All threads of the CTA call it.
+template <int D, int C>
+MGK_DEV int decide(BatchRep& R, rng::Mt* mt) {
+    __shared__ int s_act, s_blk, s_sel;
+    __shared__ double s_target;
+    __shared__ dd sh[32];
+    __shared__ dd s_before;
+    BatchCtl* c = R.ctl;
+    if (threadIdx.x == 0) {
+        dd tot = {0.0, 0.0};
+        int nun = 0;
+        for (int b = 0; b < R.ncta; ++b) {
+            tot = dd_add(tot, R.chunk_sum[b]);
+            nun += R.chunk_unst[b];
+        }
+        int act = ACT_END;
+        double target = 0.0;
+        const unsigned long long now = global_ns();
+        if (c->t_start_ns == 0) c->t_start_ns = now;
+        if (now - c->t_start_ns > c->limit_ns) {
+            act = ACT_STOP;  // wall-time bound of one run call (a sustained avalanche never ends)
+            c->status = 2;
+            c->done = 1;
+        } else if (!R.p.kmc_mode && nun > 0) {
+            act = ACT_CASCADE;
+            c->ccount = 0;
+        } else {
+            if (c->cascade_active) {
+                c->cascade_active = 0;
+                c->cascades++;
+            }
+            const double Rv = tot.hi + tot.lo;
+            if (Rv > 0.0) {
+                const double u1 = rng::uniform(mt, 0.0, 1.0);
+                const double tw = __ddiv_rn(-log(u1), Rv);
+                if (tw < c->remaining) {
+                    c->time = __dadd_rn(c->time, tw);
+                    c->eps_macro[c->ci] = __dadd_rn(c->eps_macro[c->ci], __dmul_rn(1.0, __dmul_rn(c->strain_rate, tw)));
+                    c->remaining = __dsub_rn(c->remaining, tw);
+                    target = __dmul_rn(rng::uniform(mt, 0.0, 1.0), Rv);
+                    act = ACT_EVENT;
+                }
+            }
+            if (act == ACT_END) {
+                c->eps_macro[c->ci] = __dadd_rn(c->eps_macro[c->ci], __dmul_rn(1.0, __dmul_rn(c->strain_rate, c->remaining)));
+                c->time = __dadd_rn(c->time, c->remaining);
+                c->remaining = 0.0;
+            }
+        }
+        s_act = act;
+        s_target = target;
+        s_blk = 0x7fffffff;
+        s_sel = 0x7fffffff;
+        c->action = act;
+    }
+    __syncthreads();
+    if (s_act != ACT_EVENT) return s_act;
+    // selection: the chunk holding the crossing, then the mode inside it
+    const double target = s_target;
+    const int nc = R.ncta;
+    const int seg = (nc + blockDim.x - 1) / blockDim.x;
+    const int b0 = threadIdx.x * seg, b1 = min(nc, b0 + seg);
+    dd mine = {0.0, 0.0};
+    for (int b = b0; b < b1; ++b) mine = dd_add(mine, R.chunk_sum[b]);
+    dd run = block_excl_scan(mine, sh, nullptr);
+    int my_blk = -1;
+    for (int b = b0; b < b1; ++b) {
+        const dd nx = dd_add(run, R.chunk_sum[b]);
+        if (dd_ge(nx, target)) {
+            my_blk = b;
+            atomicMin(&s_blk, b);
+            break;
+        }
+        run = nx;
+    }
+    __syncthreads();
+    const int cb = s_blk;
+    long cand = -1;
+    double cmargin = 0.0;
+    if (cb != 0x7fffffff) {
+        if (my_blk == cb) s_before = run;
+        __syncthreads();
+        const long NM = R.s.NM;
+        const long m0 = NM * cb / nc, m1 = NM * (cb + 1) / nc;
+        const long per = (m1 - m0 + blockDim.x - 1) / blockDim.x;
+        const long r0 = m0 + threadIdx.x * per, r1 = min(m1, r0 + per);
+        dd ms = {0.0, 0.0};
+        for (long i = r0; i < r1; ++i) {
+            bool inc;
+            const double r = rate_of(R.p, R.s.Q[i], &inc);
+            if (inc) ms = dd_add_d(ms, r);
+        }
+        dd pr = dd_add(s_before, block_excl_scan(ms, sh, nullptr));
+        for (long i = r0; i < r1; ++i) {
+            bool inc;
+            const double r = rate_of(R.p, R.s.Q[i], &inc);
+            if (!inc) continue;
+            const dd nx = dd_add_d(pr, r);
+            if (dd_ge(nx, target)) {
+                cand = i;
+                const double below = target - (pr.hi + pr.lo), above = (nx.hi + nx.lo) - target;
+                cmargin = fmin(below, above) / fmax(target, 1e-300);
+                atomicMin(&s_sel, (int)i);
+                break;
+            }
+            pr = nx;
+        }
+        __syncthreads();
+        if (cand >= 0 && cand == s_sel && cmargin < c->min_margin) c->min_margin = cmargin;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long k = s_sel;
+        if (k == 0x7fffffff) {
+            k = -1;
+            c->fallbacks++;
+            if (cb != 0x7fffffff)
+                for (long i = R.s.NM * (cb + 1) / nc; i < R.s.NM; ++i) {
+                    bool inc;
+                    rate_of(R.p, R.s.Q[i], &inc);
+                    if (inc) {
+                        k = i;
+                        break;
+                    }
+                }
+            if (k < 0)
+                for (int b = 0; b < nc; ++b) k = max(k, (long)R.chunk_last[b]);
+        }
+        if (k >= 0) {
+            const bool instab = R.s.Q[k] <= R.p.threshold;
+            apply_flip<D, C>(R.s, R.p, k, c->time, nullptr);
+            redraw_dev<C>(R, mt, k);
+            c->seq_instab = instab ? c->seq_instab + 1 : 0;
+            if (c->sel_log_len < c->sel_log_cap) R.sel_log[c->sel_log_len++] = (int)k;
+        }
+    }
+    __syncthreads();
+    return ACT_EVENT;
+}
+
+// bitonic sort of (key, mode) in shared memory by one CTA (n <= cap)
+MGK_DEV void cta_sort(double* keys, int* modes, int n, unsigned char* smem, size_t smem_bytes) {
+    int npow2 = 1;
+    while (npow2 < n) npow2 <<= 1;
+    const bool in_smem = (size_t)npow2 * 12 <= smem_bytes;
+    double* k = in_smem ? reinterpret_cast<double*>(smem) : keys;
+    int* m = in_smem ? reinterpret_cast<int*>(smem + (size_t)npow2 * 8) : modes;
+    if (in_smem) {
+        for (int i = threadIdx.x; i < npow2; i += blockDim.x) {
+            k[i] = i < n ? keys[i] : INFINITY;
+            m[i] = i < n ? modes[i] : 0x7fffffff;
+        }
+    } else {
+        for (int i = n + threadIdx.x; i < npow2; i += blockDim.x) {
+            k[i] = INFINITY;
+            m[i] = 0x7fffffff;
+        }
+    }
+    __syncthreads();
+    for (int size = 2; size <= npow2; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < npow2; i += blockDim.x) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const bool sw = up ? key_less(k[j], m[j], k[i], m[i]) : key_less(k[i], m[i], k[j], m[j]);
+                    if (sw) {
+                        const double tk = k[i];
+                        k[i] = k[j];
+                        k[j] = tk;
+                        const int tm = m[i];
+                        m[i] = m[j];
+                        m[j] = tm;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    if (in_smem)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) modes[i] = m[i];
+    __syncthreads();
+}
+
+template <int D, int C>
+MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem_bytes) {
+    __shared__ LsArgs s_ls;
+    __shared__ rng::Mt s_mt;
+    __shared__ int s_flag;
+    BatchCtl* c = R.ctl;
+    const GridBar gb{R.bar, (unsigned)R.ncta, R.bar + 2};
+    if (rank == 0) {
+        for (int i = threadIdx.x; i < 624; i += blockDim.x) s_mt.mt[i] = R.mt->mt[i];
+        if (threadIdx.x == 0) s_mt.idx = R.mt->idx;
+        __syncthreads();
+    }
+    bool ok = true;
+    if (vld(&c->need_initial_solve)) {
+        ok = group_solve<D>(R, rank, gb, smem, &s_ls);
+        if (ok && rank == 0 && threadIdx.x == 0) {
+            c->need_initial_solve = 0;
+            c->remaining = __dadd_rn(c->remaining, c->dt_step);
+        }
+        ok = ok && grid_sync(gb);
+    }
+    while (ok) {
+        if (vld(&c->done)) break;
+        sweep_chunk<D, C>(R, rank, c->time);
+        if (!grid_sync(gb)) break;
+        if (rank == 0) decide<D, C>(R, &s_mt);
+        if (!grid_sync(gb)) break;
+        const int act = vld(&c->action);
+        if (act == ACT_STOP) break;
+        if (act == ACT_EVENT) {
+            if (!group_solve<D>(R, rank, gb, smem, &s_ls)) break;
+            if (rank == 0 && threadIdx.x == 0) {
+                c->events_done++;
+                c->events_total++;
+                if (c->seq_instab > c->max_seq) {
+                    c->status = 1;
+                    c->done = 1;
+                }
+                if (c->events_done >= c->max_events) c->done = 1;
+            }
+        } else if (act == ACT_CASCADE) {
+            // collect the lowest-Q unstable mode of every unstable voxel
+            const long v0 = (long)R.s.N * rank / R.ncta, v1 = (long)R.s.N * (rank + 1) / R.ncta;
+            for (long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+                double best = 0.0;
+                int bm = -1;
+                for (int m = 0; m < R.s.M; ++m) {
+                    const double q = R.s.Q[v * R.s.M + m];
+                    if (q < R.p.threshold && (bm < 0 || q < best)) {
+                        best = q;
+                        bm = m;
+                    }
+                }
+                if (bm >= 0) {
+                    const int slot = atomicAdd(&c->ccount, 1);
+                    R.ckeys[slot] = best;
+                    R.cmodes[slot] = (int)(v * R.s.M + bm);
+                }
+            }
+            if (!grid_sync(gb)) break;
+            if (rank == 0) {
+                const int n = vld(&c->ccount);
+                cta_sort(R.ckeys, R.cmodes, n, smem, smem_bytes);
+                if (threadIdx.x == 0) {
+                    for (int f = 0; f < n; ++f) {
+                        const long k = R.cmodes[f];
+                        apply_flip<D, C>(R.s, R.p, k, c->time, nullptr);
+                        redraw_dev<C>(R, &s_mt, k);
+                    }
+                    c->cascade_flips += n;
+                    c->cascade_batches++;
+                    c->cascade_active = 1;
+                    if (c->cascade_batches > c->cascade_limit) {  // run_cascade's batch limit (:556)
+                        c->cascades++;
+                        c->cascade_batches = 0;
+                    }
+                }
+            }
+            if (!grid_sync(gb)) break;
+            if (!group_solve<D>(R, rank, gb, smem, &s_ls)) break;
+        } else {
+            // end of interval: mixed-BC loop, then the next interval
+            for (;;) {
+                if (!group_solve<D>(R, rank, gb, smem, &s_ls)) {
+                    ok = false;
+                    break;
+                }
+                if (rank == 0 && threadIdx.x == 0) {
+                    double err[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, emax = 0.0;
+                    for (int t = 0; t < c->n_targets; ++t) {
+                        const double e = c->tv[t] - c->sig_macro[c->tflat[t]];
+                        err[c->tflat[t]] = e;
+                        emax = fmax(emax, fabs(e));
+                    }
+                    int stop = emax < c->mixed_tol;
+                    if (!stop) {
+                        double tr = 0.0;
+                        for (int a = 0; a < D; ++a) tr += err[a * D + a];
+                        for (int t = 0; t < c->n_targets; ++t) {
+                            const int k = c->tflat[t];
+                            c->eps_macro[k] += (err[k] - c->na * tr * (c->tdiag[t] ? 1.0 : 0.0)) / c->Ea;
+                        }
+                        if (++c->mixed_it >= c->mixed_max_iter) stop = 1;
+                    }
+                    if (stop) {
+                        c->mixed_it = 0;
+                        c->elastic_done++;
+                        c->elastic_steps++;
+                        if (c->elastic_done >= c->n_global_steps) c->done = 1;
+                        else c->remaining = __dadd_rn(c->remaining, c->dt_step);
+                    }
+                    s_flag = stop;
+                    c->action = stop ? 0 : ACT_END;
+                }
+                if (!grid_sync(gb)) {
+                    ok = false;
+                    break;
+                }
+                if (vld(&c->action) == 0) break;
+            }
+            if (!ok) break;
+        }
+        if (!grid_sync(gb)) break;
+    }
+    if (rank == 0) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 624; i += blockDim.x) R.mt->mt[i] = s_mt.mt[i];
+        if (threadIdx.x == 0) R.mt->idx = s_mt.idx;
+    }
+}
+
+__global__ void __launch_bounds__(256, 1) batch_kernel(BatchRep* reps, const int2* map, size_t smem_bytes) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int2 m = map[blockIdx.x];
+    BatchRep& R = reps[m.x];
+    if (R.s.D == 2) run_replica<2, 2>(R, m.y, smem, smem_bytes);
+    else if (R.C == 2) run_replica<3, 2>(R, m.y, smem, smem_bytes);
+    else run_replica<3, 6>(R, m.y, smem, smem_bytes);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+#define BCK(x)                                                                                  \
+    do {                                                                                        \
+        cudaError_t e_ = (x);                                                                   \
+        if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* const* E, const double* const* nu) {
+    if (n < 1) throw std::invalid_argument("empty batch");
+    for (int r = 0; r < n; ++r) eng_.emplace_back(new KmcEngine(params[r], E[r], nu[r]));
+    BCK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // dynamic shared memory: the largest LS need, and room for a 4096-entry sort
+    smem_ = 4096 * 12;
+    for (auto& e : eng_) smem_ = std::max(smem_, (size_t)2 * e->ls_->args_.smem_half);
+    BCK(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
+    int per_sm = 0;
+    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 256, smem_));
+    if (per_sm < 1) throw std::runtime_error("batch kernel does not fit on an SM");
+    const int budget = per_sm * nsm;
+    if (n > budget) throw std::invalid_argument("more replicas than co-resident CTAs");
+    // CTA groups sized by work per event (modes + LS voxels), within the budget
+    std::vector<double> work(n);
+    double tot = 0.0;
+    for (int r = 0; r < n; ++r) {
+        work[r] = (double)eng_[r]->NM_ + 24.0 * eng_[r]->N_;
+        tot += work[r];
+    }
+    ncta_.assign(n, 1);
+    int used = n;
+    for (int r = 0; r < n; ++r) {
+        const int lim = std::max(1, std::min(eng_[r]->ls_->grid_, 160));
+        ncta_[r] = std::max(1, std::min(lim, (int)std::floor(budget * work[r] / tot)));
+    }
+    used = 0;
+    for (int r = 0; r < n; ++r) used += ncta_[r];
+    while (used > budget) {
+        int big = 0;
+        for (int r = 1; r < n; ++r)
+            if (ncta_[r] > ncta_[big]) big = r;
+        if (ncta_[big] <= 1) break;
+        --ncta_[big];
+        --used;
+    }
+    total_ctas_ = used;
+    // per-replica device scratch
+    std::vector<BatchRep> reps(n);
+    std::vector<int2> map;
+    for (int r = 0; r < n; ++r) {
+        KmcEngine& e = *eng_[r];
+        BatchRep& R = reps[r];
+        R.s = e.dev_;
+        R.p = e.phys_;
+        R.ls = e.ls_->args_;
+        R.bg = rng::Barrier{e.bar_.type, e.bar_.mean, e.bar_.std_val, e.bar_.min_cutoff, e.bar_.max_cutoff, e.bar_.loc,
+                            e.bar_.scale, e.bar_.epsilon, e.bar_.ratio};
+        R.gamma0 = e.p_.gamma0;
+        R.redraw_dir = e.p_.redraw_directions;
+        R.redraw_bar = e.p_.redraw_barriers;
+        R.C = e.C_;
+        R.ncta = ncta_[r];
+        auto alloc = [&](void** p, size_t b) {
+            BCK(cudaMalloc(p, b));
+            owned_.push_back(*p);
+        };
+        alloc((void**)&R.bar, 4 * sizeof(unsigned));
+        alloc((void**)&R.chunk_sum, sizeof(dd) * R.ncta);
+        alloc((void**)&R.chunk_unst, sizeof(int) * R.ncta);
+        alloc((void**)&R.chunk_last, sizeof(int) * R.ncta);
+        int npow2 = 1;
+        while (npow2 < e.N_) npow2 <<= 1;
+        alloc((void**)&R.ckeys, sizeof(double) * npow2);
+        alloc((void**)&R.cmodes, sizeof(int) * npow2);
+        R.ccap = npow2;
+        alloc((void**)&R.mt, sizeof(rng::Mt));
+        alloc((void**)&R.ctl, sizeof(BatchCtl));
+        alloc((void**)&R.sel_log, sizeof(int) * kSelLog);
+        alloc((void**)&R.ls.partials, sizeof(double) * kMaxPartials * R.ncta);
+        alloc((void**)&R.ls.result, sizeof(LsResult));
+        R.ls.bar = R.bar;
+        R.ls.err = R.bar + 2;
+        BCK(cudaMemset(R.bar, 0, 4 * sizeof(unsigned)));
+        for (int k = 0; k < R.ncta; ++k) map.push_back(make_int2(r, k));
+    }
+    alloc_reps_ = nullptr;
+    BCK(cudaMalloc((void**)&alloc_reps_, sizeof(BatchRep) * n));
+    BCK(cudaMemcpy(alloc_reps_, reps.data(), sizeof(BatchRep) * n, cudaMemcpyHostToDevice));
+    BCK(cudaMalloc((void**)&map_, sizeof(int2) * map.size()));
+    BCK(cudaMemcpy(map_, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice));
+    reps_host_ = reps;
+    first_run_.assign(n, 1);
+    remaining_.assign(n, 0.0);
+}
+
+BatchEngine::~BatchEngine() {
+    if (st_) cudaStreamSynchronize(st_);
+    for (void* p : owned_) cudaFree(p);
+    cudaFree(alloc_reps_);
+    cudaFree(map_);
+    eng_.clear();
+    if (st_) cudaStreamDestroy(st_);
+}
+
+static void mt_from_host(const std::mt19937& g, rng::Mt* out) {
+    std::ostringstream os;
+    os << g;
+    std::istringstream is(os.str());
+    unsigned long v;
+    for (int i = 0; i < 624; ++i) {
+        is >> v;
+        out->mt[i] = (unsigned)v;
+    }
+    is >> v;
+    out->idx = (int)v;
+    out->pad = 0;
+}
+
+static void mt_to_host(const rng::Mt& m, std::mt19937* g) {
+    std::ostringstream os;
+    for (int i = 0; i < 624; ++i) os << m.mt[i] << " ";
+    os << m.idx;
+    std::istringstream is(os.str());
+    is >> *g;
+}
+
+mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, double* elapsed_ms) {
+    const int n = (int)eng_.size();
+    try {
+        for (int r = 0; r < n; ++r) {
+            KmcEngine& e = *eng_[r];
+            const mgk_run_params& p = rp[r];
+            const int D = e.D_;
+            BatchCtl c{};
+            c.time = e.time_;
+            std::memcpy(c.eps_macro, e.eps_macro_, sizeof(c.eps_macro));
+            std::memcpy(c.sig_macro, e.sig_macro_, sizeof(c.sig_macro));
+            for (int k = 0; k < 3; ++k) c.w[k] = e.ls_->w_[k];
+            c.remaining = first_run_[r] ? 0.0 : remaining_[r];
+            c.dt_step = std::fabs(p.step_size) / e.p_.strain_rate;
+            c.strain_rate = e.p_.strain_rate;
+            c.sum_two_mu = e.ls_->sum_two_mu_;
+            double Es = 0.0, ns = 0.0;
+            for (double v : e.E_) Es += v;
+            for (double v : e.nu_) ns += v;
+            c.Ea = Es / e.E_.size();
+            c.na = ns / e.nu_.size();
+            c.mixed_tol = p.mixed_tol;
+            c.mixed_max_iter = p.mixed_max_iter;
+            c.ls_tol = e.p_.ls_tol;
+            c.ls_max_iter = e.p_.ls_max_iter;
+            c.n_targets = p.n_targets;
+            for (int t = 0; t < p.n_targets; ++t) {
+                c.tflat[t] = p.target_i[t] * D + p.target_j[t];
+                c.tdiag[t] = p.target_i[t] == p.target_j[t];
+                c.tv[t] = p.target_v[t];
+            }
+            c.ci = p.comp_i * D + p.comp_j;
+            c.n_global_steps = p.n_global_steps;
+            c.elastic_done = 0;
+            c.max_seq = (int)(p.max_kmc_steps_pct * (double)e.N_);
+            c.need_initial_solve = first_run_[r];
+            c.max_events = max_events > 0 ? max_events : (1LL << 62);
+            c.cascade_limit = p.max_cascade_batches > 0 ? p.max_cascade_batches : e.N_;
+            c.min_margin = 1.0;
+            c.sel_log_cap = kSelLog;
+            c.t_start_ns = 0;
+            c.limit_ns = (unsigned long long)(time_limit_s_ * 1e9);
+            BCK(cudaMemcpyAsync(reps_host_[r].ctl, &c, sizeof(BatchCtl), cudaMemcpyHostToDevice, st_));
+            rng::Mt mt;
+            mt_from_host(e.rng_, &mt);
+            BCK(cudaMemcpyAsync(reps_host_[r].mt, &mt, sizeof(rng::Mt), cudaMemcpyHostToDevice, st_));
+            BCK(cudaMemsetAsync(reps_host_[r].bar, 0, 4 * sizeof(unsigned), st_));
+            BCK(cudaStreamSynchronize(st_));
+        }
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, st_);
+        void* args[] = {&alloc_reps_, &map_, &smem_};
+        BCK(cudaLaunchCooperativeKernel((const void*)batch_kernel, dim3(total_ctas_), dim3(256), args, smem_, st_));
+        cudaEventRecord(e1, st_);
+        BCK(cudaStreamSynchronize(st_));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (elapsed_ms) *elapsed_ms = ms;
+        mgk_status st = MGK_OK;
+        last_.assign(n, BatchStats{});
+        for (int r = 0; r < n; ++r) {
+            KmcEngine& e = *eng_[r];
+            BatchCtl c;
+            unsigned bar[4];
+            rng::Mt mt;
+            BCK(cudaMemcpy(&c, reps_host_[r].ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost));
+            BCK(cudaMemcpy(bar, reps_host_[r].bar, sizeof(bar), cudaMemcpyDeviceToHost));
+            BCK(cudaMemcpy(&mt, reps_host_[r].mt, sizeof(rng::Mt), cudaMemcpyDeviceToHost));
+            if (bar[2]) {
+                last_error = "device wait timed out in the batched kernel";
+                st = MGK_DEVICE_TIMEOUT;
+            }
+            // hand the state back to the replica's engine (host mirrors)
+            e.time_ = c.time;
+            std::memcpy(e.eps_macro_, c.eps_macro, sizeof(c.eps_macro));
+            std::memcpy(e.sig_macro_, c.sig_macro, sizeof(c.sig_macro));
+            for (int k = 0; k < 3; ++k) e.ls_->w_[k] = c.w[k], e.ls_->asym_dev2_[k] = 0.0;
+            mt_to_host(mt, &e.rng_);
+            first_run_[r] = 0;
+            remaining_[r] = c.remaining;
+            BatchStats& b = last_[r];
+            b.events = c.events_done;
+            b.cascades = c.cascades + (c.cascade_active ? 1 : 0);
+            b.cascade_flips = c.cascade_flips;
+            b.ls_solves = c.ls_solves;
+            b.ls_iters = c.ls_iters;
+            b.elastic_steps = c.elastic_steps;
+            b.fallbacks = c.fallbacks;
+            b.min_margin = c.min_margin;
+            b.terminated = c.status;
+            if (c.status == 2 && st == MGK_OK) {
+                last_error = "batched run stopped at its time limit";
+                st = MGK_TIME_LIMIT;
+            }
+            b.ncta = ncta_[r];
+            b.sel.resize(c.sel_log_len);
+            if (c.sel_log_len)
+                BCK(cudaMemcpy(b.sel.data(), reps_host_[r].sel_log, sizeof(int) * c.sel_log_len, cudaMemcpyDeviceToHost));
+            e.stats_.thermal_events += c.events_done;
+            e.stats_.ls_solves += c.ls_solves;
+            e.stats_.ls_iters += c.ls_iters;
+        }
+        return st;
+    } catch (const std::exception& ex) {
+        last_error = ex.what();
+        return MGK_CUDA_ERROR;
+    }
+}
+
+}  // namespace mgk

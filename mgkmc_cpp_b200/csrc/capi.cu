@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "../../include/mgkmc_b200.h"
+#include "batch.cuh"
 #include "engine.cuh"
 #include "ls.cuh"
 
@@ -36,6 +37,10 @@ struct mgk_ls {
 
 struct mgk_kmc {
     mgk::KmcEngine* eng = nullptr;
+};
+
+struct mgk_batch {
+    mgk::BatchEngine* b = nullptr;
 };
 
 extern "C" {
@@ -203,6 +208,80 @@ mgk_status mgk_kmc_get_profile(mgk_kmc* h, double* out, double* lat, long long l
     if (lat)
         for (long long i = 0; i < lat_cap && i < (long long)p.event_us.size(); ++i) lat[i] = p.event_us[i];
     return MGK_OK;
+}
+
+mgk_status mgk_batch_create(mgk_batch** out, int n, const mgk_kmc_params* params, const double* const* E,
+                            const double* const* nu) {
+    if (!out || !params || !E || !nu || n < 1) return fail(MGK_BAD_ARG, "null argument or empty batch");
+    *out = nullptr;
+    for (int r = 0; r < n; ++r) {
+        if (!E[r] || !nu[r]) return fail(MGK_BAD_ARG, "null field");
+        if (params[r].barrier_type < 0 || params[r].barrier_type > 3) return fail(MGK_BAD_ARG, "unknown barrier type");
+    }
+    mgk_batch* h = new (std::nothrow) mgk_batch;
+    if (!h) return fail(MGK_OOM, "host allocation failed");
+    try {
+        h->b = new mgk::BatchEngine(n, params, E, nu);
+    } catch (const std::exception& e) {
+        delete h;
+        return from_exception(e);
+    }
+    *out = h;
+    return MGK_OK;
+}
+
+mgk_status mgk_batch_run(mgk_batch* h, const mgk_run_params* rp, long long max_events, double* elapsed_ms) {
+    if (!h || !rp) return fail(MGK_BAD_ARG, "null argument");
+    for (int r = 0; r < h->b->size(); ++r) {
+        const int D = h->b->replica(r)->D();
+        const mgk_run_params& p = rp[r];
+        if (p.n_targets < 0 || p.n_targets > 9) return fail(MGK_BAD_ARG, "n_targets out of range");
+        if (p.comp_i < 0 || p.comp_i >= D || p.comp_j < 0 || p.comp_j >= D) return fail(MGK_BAD_ARG, "bad driving component");
+        for (int t = 0; t < p.n_targets; ++t)
+            if (p.target_i[t] < 0 || p.target_i[t] >= D || p.target_j[t] < 0 || p.target_j[t] >= D)
+                return fail(MGK_BAD_ARG, "bad mixed target component");
+    }
+    mgk_status s = h->b->run(rp, max_events, elapsed_ms);
+    if (s != MGK_OK) g_err = h->b->last_error;
+    return s;
+}
+
+mgk_status mgk_batch_stats(mgk_batch* h, int replica, double* out, int* sel, long long sel_cap, long long* sel_len) {
+    if (!h || !out || replica < 0 || replica >= h->b->size()) return fail(MGK_BAD_ARG, "bad argument");
+    const mgk::BatchStats& b = h->b->stats(replica);
+    double v[10] = {(double)b.events, (double)b.cascades, (double)b.cascade_flips, (double)b.ls_solves, (double)b.ls_iters,
+                    (double)b.elastic_steps, (double)b.fallbacks, b.min_margin, (double)b.terminated, (double)b.ncta};
+    std::memcpy(out, v, sizeof(v));
+    if (sel)
+        for (long long i = 0; i < sel_cap && i < (long long)b.sel.size(); ++i) sel[i] = b.sel[i];
+    if (sel_len) *sel_len = (long long)b.sel.size();
+    return MGK_OK;
+}
+
+mgk_status mgk_batch_get_field(mgk_batch* h, int replica, int field, double* dst, long long* count) {
+    if (!h || replica < 0 || replica >= h->b->size()) return fail(MGK_BAD_ARG, "bad argument");
+    mgk::KmcEngine* e = h->b->replica(replica);
+    mgk_status s = e->get_field(field, dst, count);
+    if (s != MGK_OK) g_err = e->last_error;
+    return s;
+}
+
+mgk_status mgk_batch_get_macro(mgk_batch* h, int replica, double* out, int n) {
+    if (!h || !out || replica < 0 || replica >= h->b->size()) return fail(MGK_BAD_ARG, "bad argument");
+    h->b->replica(replica)->get_macro(out, n);
+    return MGK_OK;
+}
+
+mgk_status mgk_batch_set_time_limit(mgk_batch* h, double seconds) {
+    if (!h || !(seconds > 0.0) || seconds > 3600.0) return fail(MGK_BAD_ARG, "time limit outside (0, 3600] s");
+    h->b->set_time_limit(seconds);
+    return MGK_OK;
+}
+
+void mgk_batch_destroy(mgk_batch* h) {
+    if (!h) return;
+    delete h->b;
+    delete h;
 }
 
 void mgk_kmc_destroy(mgk_kmc* h) {

@@ -39,7 +39,11 @@ struct EngineProfile {
     std::vector<double> event_us;  // host wall time per thermal event
 };
 
+class BatchEngine;
+
 class KmcEngine {
+    friend class BatchEngine;
+
 public:
     KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu);
     ~KmcEngine();

@@ -64,7 +64,11 @@ struct LsArgs {
     FftAxis ax[3];         // per axis (x, y, z)
 };
 
+class BatchEngine;
+
 class LsSolver {
+    friend class BatchEngine;
+
 public:
     // dims: {nx, ny} (D=2) or {nx, ny, nz}; E, nu host arrays of N values.
     LsSolver(int D, const int* dims, bool plane_stress, double pixel, const double* E, const double* nu, cudaStream_t stream);

@@ -20,6 +20,13 @@ correlation lengths and coefficients of variation of the benchmark cases.
 * ``hetero3d_64``  -- 3D 64^3, lognormal E (CoV 0.15, correlation 3), M = 100
   random deviatoric 3D modes (system.3d_barriers), z tension.
 * ``hetero3d_16``  -- the 3D case at 16^3 with M = 20 (parity-test size).
+* ``ens2d_64``, ``ens2d_128``, ``ens2d_512``, ``ens3d_32``, ``ens3d_48``,
+  ``ens3d_96`` -- replicas of the batched ensemble: lognormal E whose CoV is
+  drawn uniformly from [0.05, 0.2] by the replica's seed (correlation length 4
+  voxels in 2D, 3 in 3D), the reference's default barriers, M = 18 in 2D and
+  M = 100 random deviatoric modes in 3D.  ``ensemble()`` lists the 64-replica
+  mix: 16 each of 2D 64^2, 128^2, 512^2 and 16 3D replicas (5 of 32^3, 5 of
+  48^3, 6 of 96^3), seeds 0..63.
 """
 from __future__ import annotations
 
@@ -93,6 +100,26 @@ WORKLOADS = {
     "hetero3d_64": dict(dim="3d", nx=64, ny=64, nz=64, M=100, b3="true", hetero=(0.15, 3.0), **_T3, **_B_REF),
     "hetero3d_16": dict(dim="3d", nx=16, ny=16, nz=16, M=20, b3="true", hetero=(0.15, 3.0), **_T3, **_B_DF1),
 }
+for _n in (64, 128, 512):
+    WORKLOADS["ens2d_%d" % _n] = dict(dim="2d", nx=_n, ny=_n, nz=1, M=18, b3="false", hetero=("draw", 4.0), **_T2,
+                                      **_B_REF)
+for _n in (32, 48, 96):
+    WORKLOADS["ens3d_%d" % _n] = dict(dim="3d", nx=_n, ny=_n, nz=_n, M=100, b3="true", hetero=("draw", 3.0), **_T3,
+                                      **_B_REF)
+
+ENSEMBLE = ["ens2d_64"] * 16 + ["ens2d_128"] * 16 + ["ens2d_512"] * 16 + ["ens3d_32"] * 5 + ["ens3d_48"] * 5 + \
+    ["ens3d_96"] * 6
+
+
+def ensemble_cov(seed: int) -> float:
+    """CoV of an ensemble replica's modulus field: uniform in [0.05, 0.2]."""
+    return float(np.random.default_rng(1000 + seed).uniform(0.05, 0.2))
+
+
+def ensemble(directory: str, names=None):
+    """(name, seed, config) of every ensemble replica; seed = position in the list."""
+    names = ENSEMBLE if names is None else names
+    return [(n, s, write_workload(n, directory, seed=s)[1]) for s, n in enumerate(names)]
 
 
 def write_workload(name: str, directory: str, seed: int = 0) -> Tuple[str, SimConfig]:
@@ -103,6 +130,8 @@ def write_workload(name: str, directory: str, seed: int = 0) -> Tuple[str, SimCo
         eblock = '    mode: "constant"\n    value: 90'
     else:
         cov, corr = w["hetero"]
+        if cov == "draw":
+            cov = ensemble_cov(seed)
         shape = (w["nx"], w["ny"], w["nz"]) if w["dim"] == "3d" else (w["nx"], w["ny"])
         E = fields.lognormal_modulus(shape, 90e9, cov, corr, seed)
         epath = os.path.join(directory, "E_%s_s%d.npy" % (name, seed))
