@@ -167,9 +167,12 @@ MGK_API void mgk_kmc_destroy(mgk_kmc* h);
  * (<= 0: until its n_global_steps elastic steps are done); rp holds n entries
  * (log and VTU fields are ignored: device-resident runs write no files);
  * elapsed_ms gets the kernel's CUDA-event time.  mgk_batch_stats fills
- * out[0..9] = {events, cascades, cascade flips, LS solves, LS iterations,
+ * out[0..15] = {events, cascades, cascade flips, LS solves, LS iterations,
  * elastic steps, selection fallbacks, smallest selection margin, terminated
- * (1 instability sequence limit, 2 time limit), CTAs of the replica} and
+ * (1 instability sequence limit, 2 time limit), CTAs of the replica, then the
+ * replica's device time in ms spent in: sweeps, decisions (selection, flip,
+ * redraw), event LS solves, cascade collection and flips, cascade LS solves,
+ * interval ends (mixed-BC loop)} and
  * copies the flat mode index of each thermal event of the last run into sel
  * (up to sel_cap; *sel_len gets the count).  A run stops every replica whose
  * run call has lasted longer than the time limit (default 60 s, set with

@@ -406,13 +406,14 @@ class KmcBatch:
         return float(ms[0])
 
     def stats(self, r: int) -> dict:
-        out = np.zeros(10)
+        out = np.zeros(16)
         cap = 1 << 16
         sel = (_lib.C.c_int * cap)()
         ln = _lib.C.c_longlong(0)
         _lib.check(_lib.lib().mgk_batch_stats(self._h, r, _lib.dptr(out), sel, cap, _lib.C.byref(ln)))
         keys = ["events", "cascades", "cascade_flips", "ls_solves", "ls_iters", "elastic_steps", "fallbacks",
-                "min_margin", "terminated", "ctas"]
+                "min_margin", "terminated", "ctas", "ms_sweep", "ms_decide", "ms_event_solve", "ms_cascade_flips",
+                "ms_cascade_solve", "ms_interval_end"]
         d = {k: float(v) for k, v in zip(keys, out)}
         d["selected"] = np.array(sel[:min(ln.value, cap)], dtype=np.int64)
         return d

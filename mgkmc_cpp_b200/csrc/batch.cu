@@ -55,6 +55,7 @@ struct BatchCtl {
     long long events_total, cascades, cascade_flips, ls_solves, ls_iters, elastic_steps, fallbacks;
     int sel_log_len, sel_log_cap;
     unsigned long long t_start_ns, limit_ns;  // device clock at the first decision; 0: unset
+    unsigned long long ph_ns[6];              // sweep, decide, event solve, cascade flips, cascade solve, interval end
 };
 
 struct BatchRep {
@@ -182,31 +183,260 @@ MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
 }
 
 // Redraw after a flip of mode k (kmc_solver.hpp:839-864 / :1854-1875) with the
-// device stream; one thread.
+// generator g, one thread: every mode of the voxel when directions or barriers
+// are redrawn, else mode k's direction and barrier.
+constexpr unsigned kAltBranch = 1u << 30;
+
 template <int C>
-MGK_DEV void redraw_dev(BatchRep& R, rng::Mt* mt, long k) {
+MGK_DEV void redraw_seq(BatchRep& R, rng::Mt* g, long k) {
     const long v = k / R.s.M;
     if (R.redraw_dir || R.redraw_bar) {
         for (int mm = 0; mm < R.s.M; ++mm) {
             const long ci = v * R.s.M + mm;
-            if (R.redraw_dir) rng::mode<C>(mt, R.gamma0, R.s.cat + ci * C);
-            if (R.redraw_bar) R.s.Q0[ci] = rng::barrier(R.bg, mt);
+            if (R.redraw_dir) rng::mode<C>(g, R.gamma0, R.s.cat + ci * C);
+            if (R.redraw_bar) R.s.Q0[ci] = rng::barrier(R.bg, g);
         }
     } else {
-        rng::mode<C>(mt, R.gamma0, R.s.cat + k * C);
-        R.s.Q0[k] = rng::barrier(R.bg, mt);
+        rng::mode<C>(g, R.gamma0, R.s.cat + k * C);
+        R.s.Q0[k] = rng::barrier(R.bg, g);
+    }
+}
+
+constexpr int kUnitsPerRound = 1024;  // modes redrawn per round of the parallel redraw
+constexpr int kSlots = 8;             // draws of one mode at most (3D: 5 polar, 1 uniform; barrier: 2)
+constexpr unsigned short kNoFit = 0xffff;
+// dynamic shared memory used by redraw_par: two flag arrays, the jump table,
+// the unit starts
+constexpr size_t kRedrawSmem = 2 * rng::kRingWords + sizeof(unsigned short) * rng::kRingWords + sizeof(long long) * kUnitsPerRound;
+
+// What one redrawn mode consumes, in the reference's order: the catalog
+// mode (2D: one polar pair; 3D: five polar pairs and one uniform) and the
+// barrier (gaussian: a polar pair; rayleigh: a uniform; modified rayleigh: a
+// rejection loop of two uniforms per attempt; the mixture: a uniform, then a
+// uniform or the rejection loop).
+struct UnitShape {
+    bool do_mode, do_bar;
+    int C, btype;
+    double ratio;
+};
+
+// Walk one mode's draws from word q over the acceptance flags; slot[] gets
+// each draw's start (the mixture's exponential branch tagged with bit 30).
+// Returns the word after the mode, or -1 when the window ends first.
+MGK_DEV long long unit_walk(const rng::MtRing* ring, const unsigned char* flagP, const unsigned char* flagR,
+                            const UnitShape& us, long long q, long long hi, int* slot) {
+    int ns = 0;
+    auto polar = [&](const unsigned char* fl) {
+        while (q + 4 <= hi && !fl[q % rng::kRingWords]) q += 4;
+        if (q + 4 > hi) return false;
+        slot[ns++] = (int)(q % rng::kRingWords);
+        q += 4;
+        return true;
+    };
+    auto uniform = [&]() {
+        if (q + 2 > hi) return false;
+        slot[ns++] = (int)(q % rng::kRingWords);
+        q += 2;
+        return true;
+    };
+    if (us.do_mode) {
+        for (int t = 0; t < (us.C == 2 ? 1 : 5); ++t)
+            if (!polar(flagP)) return -1;
+        if (us.C == 6 && !uniform()) return -1;
+    }
+    if (us.do_bar) {
+        if (us.btype == 0) {
+            if (!polar(flagP)) return -1;
+        } else if (us.btype == 1) {
+            if (!uniform()) return -1;
+        } else if (us.btype == 2) {
+            if (!polar(flagR)) return -1;
+        } else {
+            const long long qu = q;
+            if (!uniform()) return -1;
+            const double um = __dadd_rn(__dmul_rn(rng::ring_canonical(ring, qu), 1.0), 0.0);
+            if (um < us.ratio) {
+                if (!uniform()) return -1;
+                slot[ns - 1] |= (int)kAltBranch;
+            } else if (!polar(flagR)) {
+                return -1;
+            }
+        }
+    }
+    return q;
+}
+
+// Redraw after the flips of modes[0..nflips) (in flip order), by the whole
+// CTA, with the ring's stream: the same draws, in the same order, as
+// redraw_seq applied flip by flip.  Per round: refill the ring; flag every
+// attempt offset (polar acceptance, rejection acceptance) and tabulate, for
+// every offset, where a mode starting there ends (all threads); chain the
+// mode starts through that table (one thread, one lookup per mode); compute
+// the modes' values (all threads).  g is scratch for the fallback (the
+// sequential path from the program's starting state, taken if a 3D mode's
+// deviatoric part vanishes -- the reference then skips one uniform -- or a
+// mode needs more words than the ring holds).
+template <int C>
+MGK_DEV void redraw_par(BatchRep& R, rng::MtRing* ring, rng::Mt* g, const int* modes, int nflips, unsigned char* smem) {
+    __shared__ long long s_unit;
+    __shared__ int s_nu, s_fail;
+    unsigned char* flagP = smem;
+    unsigned char* flagR = smem + rng::kRingWords;
+    unsigned short* jump = reinterpret_cast<unsigned short*>(smem + 2 * rng::kRingWords);
+    long long* ustart = reinterpret_cast<long long*>(smem + 2 * rng::kRingWords + sizeof(unsigned short) * rng::kRingWords);
+    const int M = R.s.M;
+    const bool full = R.redraw_dir || R.redraw_bar;
+    UnitShape us;
+    us.do_mode = full ? R.redraw_dir != 0 : true;
+    us.do_bar = full ? R.redraw_bar != 0 : true;
+    us.C = C;
+    us.btype = R.bg.type;
+    us.ratio = R.bg.ratio;
+    const int upf = full ? M : 1;
+    const long long total = (long long)nflips * upf;
+    const bool need_r = us.do_bar && (us.btype == 2 || us.btype == 3);
+    const rng::RayleighK rk = need_r ? rng::rayleigh_k(R.bg) : rng::RayleighK{0, 0, 0, 0};
+    rng::ring_store(ring, g);  // starting state, for the fallback
+    if (threadIdx.x == 0) {
+        s_unit = 0;
+        s_fail = 0;
+    }
+    __syncthreads();
+    while (s_unit < total && !s_fail) {
+        rng::ring_refill(ring);
+        const long long p0 = ring->pos, hi = ring->hi;
+        for (long long n = p0 + threadIdx.x; n + 4 <= hi; n += blockDim.x) {
+            const int sl = (int)(n % rng::kRingWords);
+            flagP[sl] = rng::polar_accepts(ring, n);
+            if (need_r) {
+                double x;
+                flagR[sl] = rng::rayleigh_accepts(ring, n, R.bg, rk, &x);
+            }
+        }
+        __syncthreads();
+        // mode starts keep the parity of p0 (every draw takes an even number of words)
+        for (long long n = p0 + 2 * threadIdx.x; n < hi; n += 2 * blockDim.x) {
+            int sl[kSlots];
+            const long long e = unit_walk(ring, flagP, flagR, us, n, hi, sl);
+            jump[n % rng::kRingWords] = e < 0 ? kNoFit : (unsigned short)(e - n);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long o = p0, u = s_unit;
+            int nu = 0;
+            while (u < total && nu < kUnitsPerRound) {
+                const unsigned short d = jump[o % rng::kRingWords];
+                if (d == kNoFit) break;
+                ustart[nu++] = o;
+                o += d;
+                ++u;
+            }
+            if (nu == 0) s_fail = 1;  // one mode needs more than the ring holds
+            s_nu = nu;
+            ring->pos = o;
+        }
+        __syncthreads();
+        const int nu = s_nu;
+        const long long ubase = s_unit;
+        for (int j = threadIdx.x; j < nu; j += blockDim.x) {
+            const long long u = ubase + j;
+            const long f = (long)(u / upf);
+            const long k = modes[f];
+            const long ci = full ? (k / M) * M + (long)(u - (long long)f * upf) : k;
+            int rr[kSlots];
+            unit_walk(ring, flagP, flagR, us, ustart[j], hi, rr);
+            int sl = 0;
+            if (us.do_mode) {
+                if (C == 2) {
+                    double second;
+                    const double first = rng::polar_at(ring, rr[sl++], &second);
+                    const double h = __dmul_rn(0.5, R.gamma0);
+                    R.s.cat[ci * C + 0] = __dmul_rn(h, rng::scale(first, 1.0, 0.0));
+                    R.s.cat[ci * C + 1] = __dmul_rn(h, rng::scale(second, 1.0, 0.0));
+                } else {
+                    double m[10];
+                    for (int t = 0; t < 5; ++t) {
+                        double second;
+                        m[2 * t] = rng::scale(rng::polar_at(ring, rr[sl++], &second), 1.0, 0.0);
+                        m[2 * t + 1] = rng::scale(second, 1.0, 0.0);
+                    }
+                    double ms[9], G[9];
+                    for (int i = 0; i < 3; ++i)
+                        for (int jj = 0; jj < 3; ++jj) ms[i * 3 + jj] = __dmul_rn(0.5, __dadd_rn(m[i * 3 + jj], m[jj * 3 + i]));
+                    const double tr = __dadd_rn(__dadd_rn(ms[0], ms[4]), ms[8]);
+                    const double t3 = __dmul_rn(1.0 / 3.0, tr);
+                    for (int i = 0; i < 3; ++i)
+                        for (int jj = 0; jj < 3; ++jj) G[i * 3 + jj] = __dsub_rn(ms[i * 3 + jj], __dmul_rn(t3, i == jj ? 1.0 : 0.0));
+                    double sq = 0.0;
+                    for (int jj = 0; jj < 3; ++jj)
+                        for (int i = 0; i < 3; ++i) sq = __dadd_rn(sq, __dmul_rn(G[i * 3 + jj], G[i * 3 + jj]));
+                    const double nrm = __dsqrt_rn(sq);
+                    if (nrm < 1e-12) {
+                        atomicOr(&s_fail, 1);
+                        ++sl;
+                    } else {
+                        const double fct = __ddiv_rn(1.0, __dmul_rn(1.4142135623730951, nrm));
+                        for (int t = 0; t < 9; ++t) G[t] = __dmul_rn(G[t], fct);
+                        const double uu = __dadd_rn(__dmul_rn(rng::ring_canonical(ring, rr[sl++]), __dsub_rn(1.0, 1e-15)), 1e-15);
+                        const double mag = __dmul_rn(R.gamma0, __dsqrt_rn(__dmul_rn(-2.0, log(uu))));
+                        double* out = R.s.cat + ci * C;
+                        out[0] = __dmul_rn(G[0], mag);
+                        out[1] = __dmul_rn(G[4], mag);
+                        out[2] = __dmul_rn(G[8], mag);
+                        out[3] = __dmul_rn(G[1], mag);
+                        out[4] = __dmul_rn(G[2], mag);
+                        out[5] = __dmul_rn(G[5], mag);
+                    }
+                }
+            }
+            if (us.do_bar) {
+                const rng::Barrier& b = R.bg;
+                double v = 0.0;
+                if (us.btype == 0) {
+                    double unused;
+                    v = rng::scale(rng::polar_at(ring, rr[sl], &unused), b.std_val, b.mean);
+                } else if (us.btype == 1) {
+                    const double uu = __dadd_rn(__dmul_rn(rng::ring_canonical(ring, rr[sl]), 1.0), 0.0);
+                    v = __dadd_rn(b.loc, __dmul_rn(b.scale, __dsqrt_rn(__dmul_rn(-2.0, log(__dsub_rn(1.0, uu))))));
+                } else if (us.btype == 2) {
+                    rng::rayleigh_accepts(ring, rr[sl], b, rk, &v);
+                } else {
+                    const int alt = rr[sl + 1];
+                    if (alt & (int)kAltBranch) {
+                        const double uu = __dadd_rn(__dmul_rn(rng::ring_canonical(ring, alt & ~(int)kAltBranch), 1.0), 0.0);
+                        v = __dmul_rn(-b.epsilon, log(__dsub_rn(1.0, uu)));
+                    } else {
+                        rng::rayleigh_accepts(ring, alt, b, rk, &v);
+                    }
+                }
+                if (b.min_cutoff >= 0.0 && v < b.min_cutoff) v = b.min_cutoff;
+                if (b.max_cutoff >= 0.0 && v > b.max_cutoff) v = b.max_cutoff;
+                R.s.Q0[ci] = v;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_unit += nu;
+        __syncthreads();
+    }
+    if (s_fail) {
+        if (threadIdx.x == 0)
+            for (int f = 0; f < nflips; ++f) redraw_seq<C>(R, g, modes[f]);
+        __syncthreads();
+        rng::ring_load(ring, g);
     }
 }
 
 // First CTA of the group: decide the next action from the sweep; for an event
 // also select the mode and flip it.  All threads of the CTA call it.
 template <int D, int C>
-MGK_DEV int decide(BatchRep& R, rng::Mt* mt) {
+MGK_DEV int decide(BatchRep& R, rng::MtRing* ring, rng::Mt* g, unsigned char* smem) {
     __shared__ int s_act, s_blk, s_sel;
     __shared__ double s_target;
     __shared__ dd sh[32];
     __shared__ dd s_before;
+    __shared__ int s_flip;
     BatchCtl* c = R.ctl;
+    if (ring->hi - ring->pos < 16) rng::ring_refill(ring);
     if (threadIdx.x == 0) {
         dd tot = {0.0, 0.0};
         int nun = 0;
@@ -232,13 +462,13 @@ MGK_DEV int decide(BatchRep& R, rng::Mt* mt) {
             }
             const double Rv = tot.hi + tot.lo;
             if (Rv > 0.0) {
-                const double u1 = rng::uniform(mt, 0.0, 1.0);
+                const double u1 = rng::ring_uniform(ring, 0.0, 1.0);
                 const double tw = __ddiv_rn(-log(u1), Rv);
                 if (tw < c->remaining) {
                     c->time = __dadd_rn(c->time, tw);
                     c->eps_macro[c->ci] = __dadd_rn(c->eps_macro[c->ci], __dmul_rn(1.0, __dmul_rn(c->strain_rate, tw)));
                     c->remaining = __dsub_rn(c->remaining, tw);
-                    target = __dmul_rn(rng::uniform(mt, 0.0, 1.0), Rv);
+                    target = __dmul_rn(rng::ring_uniform(ring, 0.0, 1.0), Rv);
                     act = ACT_EVENT;
                 }
             }
@@ -327,15 +557,16 @@ MGK_DEV int decide(BatchRep& R, rng::Mt* mt) {
             if (k < 0)
                 for (int b = 0; b < nc; ++b) k = max(k, (long)R.chunk_last[b]);
         }
+        s_flip = (int)k;
         if (k >= 0) {
             const bool instab = R.s.Q[k] <= R.p.threshold;
             apply_flip<D, C>(R.s, R.p, k, c->time, nullptr);
-            redraw_dev<C>(R, mt, k);
             c->seq_instab = instab ? c->seq_instab + 1 : 0;
             if (c->sel_log_len < c->sel_log_cap) R.sel_log[c->sel_log_len++] = (int)k;
         }
     }
     __syncthreads();
+    if (s_flip >= 0) redraw_par<C>(R, ring, g, &s_flip, 1, smem);
     return ACT_EVENT;
 }
 
@@ -385,7 +616,10 @@ MGK_DEV void cta_sort(double* keys, int* modes, int n, unsigned char* smem, size
 template <int D, int C>
 MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem_bytes) {
     __shared__ LsArgs s_ls;
-    __shared__ rng::Mt s_mt;
+    // the replica's generator (rank 0 only) lives at the end of the dynamic
+    // shared memory, past everything the LS solve, sort and redraw use
+    rng::Mt& s_mt = *reinterpret_cast<rng::Mt*>(smem + smem_bytes);
+    rng::MtRing& s_ring = *reinterpret_cast<rng::MtRing*>(smem + smem_bytes + sizeof(rng::Mt));
     __shared__ int s_flag;
     BatchCtl* c = R.ctl;
     const GridBar gb{R.bar, (unsigned)R.ncta, R.bar + 2};
@@ -393,6 +627,7 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
         for (int i = threadIdx.x; i < 624; i += blockDim.x) s_mt.mt[i] = R.mt->mt[i];
         if (threadIdx.x == 0) s_mt.idx = R.mt->idx;
         __syncthreads();
+        rng::ring_load(&s_ring, &s_mt);
     }
     bool ok = true;
     if (vld(&c->need_initial_solve)) {
@@ -403,16 +638,28 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
         }
         ok = ok && grid_sync(gb);
     }
+    const bool timer = rank == 0 && threadIdx.x == 0;
+    unsigned long long tp = timer ? global_ns() : 0ull;
+    auto phase = [&](int k) {
+        if (timer) {
+            const unsigned long long t = global_ns();
+            c->ph_ns[k] += t - tp;
+            tp = t;
+        }
+    };
     while (ok) {
         if (vld(&c->done)) break;
         sweep_chunk<D, C>(R, rank, c->time);
         if (!grid_sync(gb)) break;
-        if (rank == 0) decide<D, C>(R, &s_mt);
+        phase(0);
+        if (rank == 0) decide<D, C>(R, &s_ring, &s_mt, smem);
         if (!grid_sync(gb)) break;
+        phase(1);
         const int act = vld(&c->action);
         if (act == ACT_STOP) break;
         if (act == ACT_EVENT) {
             if (!group_solve<D>(R, rank, gb, smem, &s_ls)) break;
+            phase(2);
             if (rank == 0 && threadIdx.x == 0) {
                 c->events_done++;
                 c->events_total++;
@@ -445,12 +692,13 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
             if (rank == 0) {
                 const int n = vld(&c->ccount);
                 cta_sort(R.ckeys, R.cmodes, n, smem, smem_bytes);
+                if (threadIdx.x == 0)
+                    for (int f = 0; f < n; ++f) apply_flip<D, C>(R.s, R.p, R.cmodes[f], c->time, nullptr);
+                __syncthreads();
+                // flips touch no other voxel's catalog or barriers, so all
+                // redraws may follow all flips (same draws, same order)
+                redraw_par<C>(R, &s_ring, &s_mt, R.cmodes, n, smem);
                 if (threadIdx.x == 0) {
-                    for (int f = 0; f < n; ++f) {
-                        const long k = R.cmodes[f];
-                        apply_flip<D, C>(R.s, R.p, k, c->time, nullptr);
-                        redraw_dev<C>(R, &s_mt, k);
-                    }
                     c->cascade_flips += n;
                     c->cascade_batches++;
                     c->cascade_active = 1;
@@ -461,7 +709,9 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
                 }
             }
             if (!grid_sync(gb)) break;
+            phase(3);
             if (!group_solve<D>(R, rank, gb, smem, &s_ls)) break;
+            phase(4);
         } else {
             // end of interval: mixed-BC loop, then the next interval
             for (;;) {
@@ -503,11 +753,13 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
                 if (vld(&c->action) == 0) break;
             }
             if (!ok) break;
+            phase(5);
         }
         if (!grid_sync(gb)) break;
     }
     if (rank == 0) {
         __syncthreads();
+        rng::ring_store(&s_ring, &s_mt);
         for (int i = threadIdx.x; i < 624; i += blockDim.x) R.mt->mt[i] = s_mt.mt[i];
         if (threadIdx.x == 0) R.mt->idx = s_mt.idx;
     }
@@ -531,6 +783,31 @@ __global__ void __launch_bounds__(256, 1) batch_kernel(BatchRep* reps, const int
         if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+// Re-plans the LS pass tiling of one replica for its group of ncta CTAs: row
+// chunks of rpb rows and column tiles of tk half-spectrum columns as large as
+// half_budget bytes of shared memory allow while every CTA still gets work,
+// so that a small group runs few, wide FFT batches instead of many narrow
+// ones.  Returns the bytes of one of the two FFT buffers.
+static size_t replan_ls(LsArgs& a, int D, int ncta, size_t half_budget) {
+    const int S = D == 2 ? 3 : 6;
+    const size_t elem = sizeof(cplx<double>);
+    auto padded = [](int n) { return (size_t)n + (size_t)(n >> 3) + 1; };
+    auto row_b = [&](int rpb) { return (size_t)((rpb * S + 1) / 2) * padded(a.nr) * elem; };
+    int rpb_max = 1;
+    while (rpb_max < a.nrows && row_b(rpb_max + 1) <= half_budget) ++rpb_max;
+    const int per_cta = (a.nrows + ncta * rpb_max - 1) / (ncta * rpb_max);
+    a.rpb = std::max(1, std::min(rpb_max, (a.nrows + ncta * per_cta - 1) / (ncta * per_cta)));
+    size_t colp = 0;
+    for (int ax = 0; ax < D - 1; ++ax) colp = std::max(colp, padded(a.dims[ax]));
+    int tk_max = 1;
+    while (tk_max < a.nh && (size_t)S * (tk_max + 1) * colp * elem <= half_budget) ++tk_max;
+    const int no_min = D == 2 ? 1 : std::min(a.dims[0], a.dims[1]);
+    const int tiles = std::max(1, (ncta + no_min - 1) / no_min);  // column tiles wanted per outer index
+    a.tk = std::max(1, std::min(tk_max, (a.nh + tiles - 1) / tiles));
+    const size_t half = std::max(row_b(a.rpb), (size_t)S * a.tk * colp * elem);
+    return (half + 127) / 128 * 128;
+}
+
 BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* const* E, const double* const* nu) {
     if (n < 1) throw std::invalid_argument("empty batch");
     for (int r = 0; r < n; ++r) eng_.emplace_back(new KmcEngine(params[r], E[r], nu[r]));
@@ -538,13 +815,11 @@ BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* cons
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    // dynamic shared memory: the largest LS need, and room for a 4096-entry sort
-    smem_ = 4096 * 12;
-    for (auto& e : eng_) smem_ = std::max(smem_, (size_t)2 * e->ls_->args_.smem_half);
-    BCK(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
-    int per_sm = 0;
-    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 256, smem_));
-    if (per_sm < 1) throw std::runtime_error("batch kernel does not fit on an SM");
+    // one CTA per SM (the kernel needs ~250 registers a thread); the dynamic
+    // shared memory holds two LS FFT buffers (or the cascade sort / redraw
+    // scratch) and, past them, the replica generator
+    const int per_sm = 1;
+    const size_t half_budget = 94 * 1024;
     const int budget = per_sm * nsm;
     if (n > budget) throw std::invalid_argument("more replicas than co-resident CTAs");
     // CTA groups sized by work per event (modes + LS voxels), within the budget
@@ -571,6 +846,20 @@ BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* cons
         --used;
     }
     total_ctas_ = used;
+    std::vector<LsArgs> plans(n);
+    smem_ = std::max((size_t)4096 * 12, kRedrawSmem);
+    for (int r = 0; r < n; ++r) {
+        plans[r] = eng_[r]->ls_->args_;
+        const size_t half = replan_ls(plans[r], eng_[r]->D_, ncta_[r], half_budget);
+        plans[r].smem_half = (int)half;
+        smem_ = std::max(smem_, 2 * half);
+    }
+    smem_ = (smem_ + 15) & ~(size_t)15;
+    const size_t smem_launch = smem_ + sizeof(rng::Mt) + sizeof(rng::MtRing);
+    BCK(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_launch));
+    int fit = 0;
+    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, batch_kernel, 256, smem_launch));
+    if (fit < 1) throw std::runtime_error("batch kernel does not fit on an SM");
     // per-replica device scratch
     std::vector<BatchRep> reps(n);
     std::vector<int2> map;
@@ -579,7 +868,7 @@ BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* cons
         BatchRep& R = reps[r];
         R.s = e.dev_;
         R.p = e.phys_;
-        R.ls = e.ls_->args_;
+        R.ls = plans[r];
         R.bg = rng::Barrier{e.bar_.type, e.bar_.mean, e.bar_.std_val, e.bar_.min_cutoff, e.bar_.max_cutoff, e.bar_.loc,
                             e.bar_.scale, e.bar_.epsilon, e.bar_.ratio};
         R.gamma0 = e.p_.gamma0;
@@ -705,7 +994,8 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
         cudaEventCreate(&e1);
         cudaEventRecord(e0, st_);
         void* args[] = {&alloc_reps_, &map_, &smem_};
-        BCK(cudaLaunchCooperativeKernel((const void*)batch_kernel, dim3(total_ctas_), dim3(256), args, smem_, st_));
+        const size_t smem_launch = smem_ + sizeof(rng::Mt) + sizeof(rng::MtRing);
+        BCK(cudaLaunchCooperativeKernel((const void*)batch_kernel, dim3(total_ctas_), dim3(256), args, smem_launch, st_));
         cudaEventRecord(e1, st_);
         BCK(cudaStreamSynchronize(st_));
         float ms = 0.f;
@@ -750,6 +1040,7 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
                 st = MGK_TIME_LIMIT;
             }
             b.ncta = ncta_[r];
+            for (int k = 0; k < 6; ++k) b.phase_ms[k] = 1e-6 * (double)c.ph_ns[k];
             b.sel.resize(c.sel_log_len);
             if (c.sel_log_len)
                 BCK(cudaMemcpy(b.sel.data(), reps_host_[r].sel_log, sizeof(int) * c.sel_log_len, cudaMemcpyDeviceToHost));

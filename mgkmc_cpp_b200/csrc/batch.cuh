@@ -17,6 +17,7 @@ struct BatchStats {
     double min_margin = 1.0;
     int terminated = 0;  // 1: instability sequence limit, 2: time limit
     int ncta = 0;
+    double phase_ms[6] = {0, 0, 0, 0, 0, 0};  // group time in sweep, decide, event solve, cascade flips, cascade solve, interval end
     std::vector<int> sel;  // flat mode index of each thermal event, in order
 };
 

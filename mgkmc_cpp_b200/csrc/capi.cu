@@ -249,8 +249,9 @@ mgk_status mgk_batch_run(mgk_batch* h, const mgk_run_params* rp, long long max_e
 mgk_status mgk_batch_stats(mgk_batch* h, int replica, double* out, int* sel, long long sel_cap, long long* sel_len) {
     if (!h || !out || replica < 0 || replica >= h->b->size()) return fail(MGK_BAD_ARG, "bad argument");
     const mgk::BatchStats& b = h->b->stats(replica);
-    double v[10] = {(double)b.events, (double)b.cascades, (double)b.cascade_flips, (double)b.ls_solves, (double)b.ls_iters,
-                    (double)b.elastic_steps, (double)b.fallbacks, b.min_margin, (double)b.terminated, (double)b.ncta};
+    double v[16] = {(double)b.events, (double)b.cascades, (double)b.cascade_flips, (double)b.ls_solves, (double)b.ls_iters,
+                    (double)b.elastic_steps, (double)b.fallbacks, b.min_margin, (double)b.terminated, (double)b.ncta,
+                    b.phase_ms[0], b.phase_ms[1], b.phase_ms[2], b.phase_ms[3], b.phase_ms[4], b.phase_ms[5]};
     std::memcpy(out, v, sizeof(v));
     if (sel)
         for (long long i = 0; i < sel_cap && i < (long long)b.sel.size(); ++i) sel[i] = b.sel[i];

@@ -160,3 +160,153 @@ MGK_DEV void mode(Mt* g, double gamma0, double* out) {
 
 }  // namespace rng
 }  // namespace mgk
+
+namespace mgk {
+namespace rng {
+
+// ---------------------------------------------------------------------------
+// The same stream, drawn by a whole CTA.  MT19937's output sequence obeys
+// x[n] = x[n-227] ^ T(x[n-624], x[n-623]) on the untempered words, so a CTA
+// extends it 227 words per parallel step into a ring in shared memory.  A
+// redraw program (the polar-method normals, uniforms and rejection draws of
+// the catalog and barrier redraws, in the reference's order) then needs, per
+// draw, only "where does the next accepted attempt start": the acceptance of
+// every attempt offset is computed in parallel, one thread walks the program
+// over those flags, and the values are computed in parallel per mode.
+constexpr int kRingGens = 8;
+constexpr int kRingWords = 624 * kRingGens;
+
+struct MtRing {
+    unsigned x[kRingWords];  // x[n % kRingWords] for n in [lo, hi)
+    long long lo, hi;        // hi and lo are multiples of 624
+    long long pos;           // next word to consume
+};
+
+MGK_DEV unsigned temper(unsigned y) {
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+MGK_DEV unsigned ring_word(const MtRing* r, long long n) { return temper(r->x[n % kRingWords]); }
+
+MGK_DEV double ring_canonical(const MtRing* r, long long n) {
+    const double lo = (double)ring_word(r, n);
+    const double hi = (double)ring_word(r, n + 1);
+    double v = __dmul_rn(__dadd_rn(lo, __dmul_rn(hi, 4294967296.0)), 5.42101086242752217e-20);
+    if (v >= 1.0) v = 0.99999999999999988898;
+    return v;
+}
+
+// all threads: ring <- generator state g (words of the current generation at
+// positions 0..623, next word at g->idx)
+MGK_DEV void ring_load(MtRing* r, const Mt* g) {
+    for (int i = threadIdx.x; i < 624; i += blockDim.x) r->x[i] = g->mt[i];
+    if (threadIdx.x == 0) {
+        r->lo = 0;
+        r->hi = 624;
+        r->pos = g->idx;
+    }
+    __syncthreads();
+}
+
+// all threads: generator state of the ring's position
+MGK_DEV void ring_store(const MtRing* r, Mt* g) {
+    const long long pos = r->pos;
+    const long long gs = pos == 0 ? 0 : ((pos - 1) / 624) * 624;  // generation holding word pos-1
+    for (int i = threadIdx.x; i < 624; i += blockDim.x) g->mt[i] = r->x[(gs + i) % kRingWords];
+    if (threadIdx.x == 0) g->idx = (int)(pos - gs);
+    __syncthreads();
+}
+
+// all threads: drop words no longer needed and extend the ring as far as it
+// holds (whole generations).
+MGK_DEV void ring_refill(MtRing* r) {
+    __shared__ long long s_lo, s_hi;
+    if (threadIdx.x == 0) {
+        const long long pos = r->pos;
+        const long long gs = pos == 0 ? 0 : ((pos - 1) / 624) * 624;
+        long long lo = r->lo;
+        const long long keep = min(gs, r->hi - 624);
+        if (keep > lo) lo = keep;
+        r->lo = lo;
+        s_lo = lo;
+        s_hi = r->hi;
+    }
+    __syncthreads();
+    const long long target = s_lo + kRingWords;
+    for (long long n0 = s_hi; n0 < target; n0 += 227) {
+        const long long n1 = min(n0 + 227, target);
+        for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+            const unsigned a = r->x[(n - 624) % kRingWords], b = r->x[(n - 623) % kRingWords];
+            const unsigned y = (a & 0x80000000u) | (b & 0x7fffffffu);
+            r->x[n % kRingWords] = r->x[(n - 227) % kRingWords] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) r->hi = target;
+    __syncthreads();
+}
+
+// one thread: a uniform in [a, b) from the ring (the caller made sure two
+// words are available)
+MGK_DEV double ring_uniform(MtRing* r, double a, double b) {
+    const double c = ring_canonical(r, r->pos);
+    r->pos += 2;
+    return __dadd_rn(__dmul_rn(c, __dsub_rn(b, a)), a);
+}
+
+// the polar attempt starting at word n: accepted?  (x from words n, n+1;
+// y from n+2, n+3)
+MGK_DEV bool polar_accepts(const MtRing* r, long long n) {
+    const double x = __dsub_rn(__dmul_rn(2.0, ring_canonical(r, n)), 1.0);
+    const double y = __dsub_rn(__dmul_rn(2.0, ring_canonical(r, n + 2)), 1.0);
+    const double r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+    return !(r2 > 1.0 || r2 == 0.0);
+}
+
+// the normals of the accepted polar attempt at word n: returns the first
+// (y * mult), *second = x * mult
+MGK_DEV double polar_at(const MtRing* r, long long n, double* second) {
+    const double x = __dsub_rn(__dmul_rn(2.0, ring_canonical(r, n)), 1.0);
+    const double y = __dsub_rn(__dmul_rn(2.0, ring_canonical(r, n + 2)), 1.0);
+    const double r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+    const double mult = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, log(r2)), r2));
+    *second = __dmul_rn(x, mult);
+    return __dmul_rn(y, mult);
+}
+
+// constants of the modified-Rayleigh rejection sampler (mod_rayleigh above)
+struct RayleighK {
+    double lo, hi, ss, cm;
+};
+
+MGK_DEV RayleighK rayleigh_k(const Barrier& b) {
+    RayleighK k;
+    k.lo = __dsub_rn(b.mean, __dmul_rn(6.0, b.std_val));
+    if (k.lo < 0.0) k.lo = 0.0;
+    k.hi = __dadd_rn(b.mean, __dmul_rn(6.0, b.std_val));
+    k.ss = __dmul_rn(__dmul_rn(2.0, b.std_val), b.std_val);
+    const double xm = __ddiv_rn(
+        __dadd_rn(b.mean, __dsqrt_rn(__dadd_rn(__dmul_rn(b.mean, b.mean), __dmul_rn(__dmul_rn(4.0, b.std_val), b.std_val)))),
+        2.0);
+    const double dm = __dsub_rn(xm, b.mean);
+    k.cm = __dmul_rn(xm, exp(__ddiv_rn(-__dmul_rn(dm, dm), k.ss)));
+    return k;
+}
+
+// the rejection attempt at word n (x from n, n+1; u from n+2, n+3): accepted?
+// *x gets the candidate
+MGK_DEV bool rayleigh_accepts(const MtRing* r, long long n, const Barrier& b, const RayleighK& k, double* xo) {
+    const double x = __dadd_rn(__dmul_rn(ring_canonical(r, n), __dsub_rn(k.hi, k.lo)), k.lo);
+    const double u = __dadd_rn(__dmul_rn(ring_canonical(r, n + 2), __dsub_rn(k.cm, 0.0)), 0.0);
+    const double d = __dsub_rn(x, b.mean);
+    const double pdf = __dmul_rn(x, exp(__ddiv_rn(-__dmul_rn(d, d), k.ss)));
+    *xo = x;
+    return u < pdf;
+}
+
+}  // namespace rng
+}  // namespace mgk
