@@ -70,6 +70,8 @@ struct BatchRep {
     dd* chunk_sum;
     int* chunk_unst;
     int* chunk_last;
+    dd* tile_sum;   // per chunk: rate sums of 32-mode tiles, tile_cap entries per chunk
+    int tile_cap;
     double* ckeys;
     int* cmodes;
     int ccap;
@@ -134,28 +136,40 @@ MGK_DEV bool group_solve(BatchRep& R, int rank, const GridBar& gb, unsigned char
     return true;
 }
 
+// Sweep of the group's rank-th chunk of modes: Q and rates of every mode
+// (update_barriers + the rate block, kmc_solver.hpp:341-410, :783-803), with
+// each warp handling 32-mode tiles: the tile's rate sum (double-double) goes
+// to tile_sum, the chunk's sum, unstable count and last included mode to the
+// chunk arrays.
 template <int D, int C>
 MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
-    __shared__ dd sd[8];
-    __shared__ int si[8], sl[8];
+    __shared__ dd sd[32];
+    __shared__ int si[32], sl[32];
     const long NM = R.s.NM;
     const long m0 = NM * rank / R.ncta, m1 = NM * (rank + 1) / R.ncta;
+    const long ntile = (m1 - m0 + 31) >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    dd* ts = R.tile_sum + (long)rank * R.tile_cap;
     dd acc = {0.0, 0.0};
     int unst = 0, last = -1;
-    for (long i = m0 + threadIdx.x; i < m1; i += blockDim.x) {
-        const int v = (int)(i / R.s.M);
-        const double q = mode_Q<D, C>(R.s, R.p, v, i, time);
-        R.s.Q[i] = q;
-        bool inc;
-        const double r = rate_of(R.p, q, &inc);
-        if (inc) {
-            last = (int)i;
-            acc = dd_add_d(acc, r);
+    for (long t = wid; t < ntile; t += nw) {
+        const long i = m0 + (t << 5) + lane;
+        dd r = {0.0, 0.0};
+        if (i < m1) {
+            const int v = (int)(i / R.s.M);
+            const double q = mode_Q<D, C>(R.s, R.p, v, i, time);
+            R.s.Q[i] = q;
+            bool inc;
+            r.hi = rate_of(R.p, q, &inc);
+            if (inc) last = (int)i;
+            if (q < R.p.threshold) ++unst;
         }
-        if (q < R.p.threshold) ++unst;
+        r = warp_dd_sum(r);
+        if (lane == 0) {
+            ts[t] = r;
+            acc = dd_add(acc, r);
+        }
     }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    acc = warp_dd_sum(acc);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         unst += __shfl_down_sync(0xffffffffu, unst, o);
@@ -170,7 +184,7 @@ MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
     if (threadIdx.x == 0) {
         dd a = {0.0, 0.0};
         int u = 0, l = -1;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        for (int w = 0; w < nw; ++w) {
             a = dd_add(a, sd[w]);
             u += si[w];
             l = max(l, sl[w]);
@@ -182,9 +196,6 @@ MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
     __syncthreads();
 }
 
-// Redraw after a flip of mode k (kmc_solver.hpp:839-864 / :1854-1875) with the
-// generator g, one thread: every mode of the voxel when directions or barriers
-// are redrawn, else mode k's direction and barrier.
 constexpr unsigned kAltBranch = 1u << 30;
 
 template <int C>
@@ -430,10 +441,10 @@ MGK_DEV void redraw_par(BatchRep& R, rng::MtRing* ring, rng::Mt* g, const int* m
 // also select the mode and flip it.  All threads of the CTA call it.
 template <int D, int C>
 MGK_DEV int decide(BatchRep& R, rng::MtRing* ring, rng::Mt* g, unsigned char* smem) {
-    __shared__ int s_act, s_blk, s_sel;
+    __shared__ int s_act, s_blk, s_sel, s_tile;
     __shared__ double s_target;
     __shared__ dd sh[32];
-    __shared__ dd s_before;
+    __shared__ dd s_before, s_tile_before;
     __shared__ int s_flip;
     BatchCtl* c = R.ctl;
     if (ring->hi - ring->pos < 16) rng::ring_refill(ring);
@@ -482,62 +493,94 @@ MGK_DEV int decide(BatchRep& R, rng::MtRing* ring, rng::Mt* g, unsigned char* sm
         s_target = target;
         s_blk = 0x7fffffff;
         s_sel = 0x7fffffff;
+        s_tile = 0x7fffffff;
         c->action = act;
     }
     __syncthreads();
     if (s_act != ACT_EVENT) return s_act;
-    // selection: the chunk holding the crossing, then the mode inside it
+    // selection (kmc_solver.hpp:817-838): the chunk holding the crossing of
+    // the cumulative rate with the target, then its 32-mode tile, then the
+    // mode, each by a fixed-order double-double prefix
     const double target = s_target;
     const int nc = R.ncta;
-    const int seg = (nc + blockDim.x - 1) / blockDim.x;
-    const int b0 = threadIdx.x * seg, b1 = min(nc, b0 + seg);
-    dd mine = {0.0, 0.0};
-    for (int b = b0; b < b1; ++b) mine = dd_add(mine, R.chunk_sum[b]);
-    dd run = block_excl_scan(mine, sh, nullptr);
-    int my_blk = -1;
-    for (int b = b0; b < b1; ++b) {
-        const dd nx = dd_add(run, R.chunk_sum[b]);
-        if (dd_ge(nx, target)) {
-            my_blk = b;
-            atomicMin(&s_blk, b);
-            break;
+    {
+        const int seg = (nc + blockDim.x - 1) / blockDim.x;
+        const int b0 = threadIdx.x * seg, b1 = min(nc, b0 + seg);
+        dd mine = {0.0, 0.0};
+        for (int b = b0; b < b1; ++b) mine = dd_add(mine, R.chunk_sum[b]);
+        dd run = block_excl_scan(mine, sh, nullptr);
+        int my_blk = -1;
+        for (int b = b0; b < b1; ++b) {
+            const dd nx = dd_add(run, R.chunk_sum[b]);
+            if (dd_ge(nx, target)) {
+                my_blk = b;
+                atomicMin(&s_blk, b);
+                break;
+            }
+            run = nx;
         }
-        run = nx;
+        __syncthreads();
+        if (my_blk >= 0 && my_blk == s_blk) s_before = run;
     }
     __syncthreads();
     const int cb = s_blk;
-    long cand = -1;
-    double cmargin = 0.0;
+    long m0 = 0, m1 = 0;
     if (cb != 0x7fffffff) {
-        if (my_blk == cb) s_before = run;
-        __syncthreads();
-        const long NM = R.s.NM;
-        const long m0 = NM * cb / nc, m1 = NM * (cb + 1) / nc;
-        const long per = (m1 - m0 + blockDim.x - 1) / blockDim.x;
-        const long r0 = m0 + threadIdx.x * per, r1 = min(m1, r0 + per);
-        dd ms = {0.0, 0.0};
-        for (long i = r0; i < r1; ++i) {
-            bool inc;
-            const double r = rate_of(R.p, R.s.Q[i], &inc);
-            if (inc) ms = dd_add_d(ms, r);
-        }
-        dd pr = dd_add(s_before, block_excl_scan(ms, sh, nullptr));
-        for (long i = r0; i < r1; ++i) {
-            bool inc;
-            const double r = rate_of(R.p, R.s.Q[i], &inc);
-            if (!inc) continue;
-            const dd nx = dd_add_d(pr, r);
+        m0 = R.s.NM * cb / nc;
+        m1 = R.s.NM * (cb + 1) / nc;
+        const long ntile = (m1 - m0 + 31) >> 5;
+        const dd* ts = R.tile_sum + (long)cb * R.tile_cap;
+        const long seg = (ntile + blockDim.x - 1) / blockDim.x;
+        const long t0 = threadIdx.x * seg, t1 = min(ntile, t0 + seg);
+        dd mine = {0.0, 0.0};
+        for (long t = t0; t < t1; ++t) mine = dd_add(mine, ts[t]);
+        dd run = dd_add(s_before, block_excl_scan(mine, sh, nullptr));
+        long my_tile = -1;
+        for (long t = t0; t < t1; ++t) {
+            const dd nx = dd_add(run, ts[t]);
             if (dd_ge(nx, target)) {
-                cand = i;
-                const double below = target - (pr.hi + pr.lo), above = (nx.hi + nx.lo) - target;
-                cmargin = fmin(below, above) / fmax(target, 1e-300);
-                atomicMin(&s_sel, (int)i);
+                my_tile = t;
+                atomicMin(&s_tile, (int)t);
                 break;
             }
-            pr = nx;
+            run = nx;
         }
         __syncthreads();
-        if (cand >= 0 && cand == s_sel && cmargin < c->min_margin) c->min_margin = cmargin;
+        if (my_tile >= 0 && my_tile == s_tile) s_tile_before = run;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32 && cb != 0x7fffffff && s_tile != 0x7fffffff) {
+        const int lane = threadIdx.x;
+        const long i = m0 + ((long)s_tile << 5) + lane;
+        bool inc = false;
+        double r = 0.0;
+        if (i < m1) r = rate_of(R.p, R.s.Q[i], &inc);
+        dd incl = {r, 0.0};
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const dd y = {__shfl_up_sync(0xffffffffu, incl.hi, o), __shfl_up_sync(0xffffffffu, incl.lo, o)};
+            if (lane >= o) incl = dd_add(y, incl);
+        }
+        dd excl = {__shfl_up_sync(0xffffffffu, incl.hi, 1), __shfl_up_sync(0xffffffffu, incl.lo, 1)};
+        if (lane == 0) excl = dd{0.0, 0.0};
+        const dd before = s_tile_before;
+        const dd nx = dd_add(before, incl);
+        const dd pr = dd_add(before, excl);
+        const unsigned hit = __ballot_sync(0xffffffffu, inc && dd_ge(nx, target));
+        const unsigned incm = __ballot_sync(0xffffffffu, inc);
+        if (lane == 0) {
+            if (hit) {
+                s_sel = (int)(m0 + ((long)s_tile << 5) + (__ffs(hit) - 1));
+            } else if (incm) {  // the tile's sum and its scan differ in the last bits: its last mode
+                s_sel = (int)(m0 + ((long)s_tile << 5) + (31 - __clz(incm)));
+                c->fallbacks++;
+            }
+        }
+        if (hit && lane == __ffs(hit) - 1) {
+            const double below = target - (pr.hi + pr.lo), above = (nx.hi + nx.lo) - target;
+            const double cmargin = fmin(below, above) / fmax(target, 1e-300);
+            if (cmargin < c->min_margin) c->min_margin = cmargin;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -545,17 +588,7 @@ MGK_DEV int decide(BatchRep& R, rng::MtRing* ring, rng::Mt* g, unsigned char* sm
         if (k == 0x7fffffff) {
             k = -1;
             c->fallbacks++;
-            if (cb != 0x7fffffff)
-                for (long i = R.s.NM * (cb + 1) / nc; i < R.s.NM; ++i) {
-                    bool inc;
-                    rate_of(R.p, R.s.Q[i], &inc);
-                    if (inc) {
-                        k = i;
-                        break;
-                    }
-                }
-            if (k < 0)
-                for (int b = 0; b < nc; ++b) k = max(k, (long)R.chunk_last[b]);
+            for (int b = 0; b < nc; ++b) k = max(k, (long)R.chunk_last[b]);
         }
         s_flip = (int)k;
         if (k >= 0) {
@@ -819,7 +852,7 @@ BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* cons
     // shared memory holds two LS FFT buffers (or the cascade sort / redraw
     // scratch) and, past them, the replica generator
     const int per_sm = 1;
-    const size_t half_budget = 94 * 1024;
+    const size_t half_budget = 92 * 1024;
     const int budget = per_sm * nsm;
     if (n > budget) throw std::invalid_argument("more replicas than co-resident CTAs");
     // CTA groups sized by work per event (modes + LS voxels), within the budget
@@ -884,6 +917,8 @@ BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* cons
         alloc((void**)&R.chunk_sum, sizeof(dd) * R.ncta);
         alloc((void**)&R.chunk_unst, sizeof(int) * R.ncta);
         alloc((void**)&R.chunk_last, sizeof(int) * R.ncta);
+        R.tile_cap = (int)((e.NM_ / R.ncta + 2 + 31) / 32);
+        alloc((void**)&R.tile_sum, sizeof(dd) * R.tile_cap * R.ncta);
         int npow2 = 1;
         while (npow2 < e.N_) npow2 <<= 1;
         alloc((void**)&R.ckeys, sizeof(double) * npow2);
