@@ -1,24 +1,39 @@
 #!/usr/bin/env python3
-"""Benchmark: KMC steps/s of the STZ-KMC + Lippmann-Schwinger step on B200.
+"""Benchmark: KMC steps/s of the STZ-KMC + Lippmann-Schwinger step on B200,
+chosen form vs plain form.
 
-One step = one thermal KMC event of run_simulation (kmc_solver.hpp:783-938):
-sweep of every (voxel, mode) barrier and rate, event selection, flip with its
-catalog/barrier redraw, and the warm-started FP64 LS re-solve; cascades and the
-end-of-interval mixed-BC solves that fall inside the timed segment are part of
-the work, as in the reference.  Default workload ``hetero2d_256`` (2D 256x256
-plane strain, seeded synthetic lognormal modulus field, CoV 0.10, correlation 4
-voxels, M = 18 modes per voxel), the single-replica heterogeneous case.  Its
-working set (~40 MB) is smaller than L2 and every step reads all of it; no L2
-flush between steps (noted in config).
+One step = one thermal KMC event of one replica's run_simulation
+(kmc_solver.hpp:783-938): sweep of every (voxel, mode) barrier and rate, event
+selection, flip with its catalog/barrier redraw, and the warm-started FP64 LS
+re-solve; cascades and the end-of-interval mixed-BC solves that fall inside
+the timed region are part of the work, as in the reference.
+
+Workload (the heterogeneous 2D case): ``hetero2d_256`` at seeds 0-3, four
+independent replicas (2D 256x256 plane strain, seeded synthetic lognormal
+modulus field, CoV 0.10, correlation 4 voxels, M = 18 modes per voxel).
+
+* ``value`` -- the chosen form: the four replicas advanced together by the
+  batched, device-resident kernel (mgk_batch_run), K thermal events each;
+  CUDA-event time of the launch.  ``e2e``: the same through the public call
+  with its host<->device copies, wall clock.
+* ``plain`` -- the drop-in form (mgk_kmc_run, one replica at a time, host RNG
+  replay), K events of seed 0, CUDA-event time of the run; its ``e2e``
+  through the public API with every step's copies.
+* ``ensemble`` (unless --no-ensemble) -- the 64-replica mixed ensemble (16 each
+  of 2D 64^2, 128^2, 512^2, 16 3D of 32^3 / 48^3 / 96^3) in one launch for a
+  fixed device time, against the plain form's per-replica rates.
+* ``cpu_baseline`` / --impl reference -- the reference's own CPU code
+  (oracle/_ref/ref_driver, compiled from the reference sources), one process
+  per replica run concurrently, on a bounded sample of the same workload.
+
+Every step reads the whole working set (~40 MB per replica, under the 126 MB
+L2), so no L2 flush is done between steps (noted in config).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-N > 1 (launched with torch.distributed.run): independent replicas, one per
-GPU, each with its own seed; no data-path collective ("replicas only"), the
-process group only times (barrier, max over ranks) and sums events.
---impl reference times the reference's own CPU implementation (the reference
-sources compiled by oracle/Makefile into oracle/_ref/ref_driver) on the same
-workload (bounded sample), rank 0 only.
+N > 1 (launched with torch.distributed.run): replicas only -- every rank runs
+its own four replicas (seeds 4*rank .. 4*rank+3); the process group only times
+(barrier, max over ranks) and sums events.
 """
 from __future__ import annotations
 
@@ -118,23 +133,37 @@ def traffic_from_profiles(workload: str):
     return float(m.group(1)) if m else None
 
 
-def run_reference(cfg_path: str, n_events: int, timeout: float = 900.0):
+def run_reference(cfg_paths, n_events: int, timeout: float = 900.0):
     """Time the reference's own CPU path (oracle/_ref/ref_driver kmc_trace):
-    the first n_events thermal events of the workload, setup excluded."""
+    the first n_events thermal events of every workload in cfg_paths, one
+    process each, all at once; setup excluded.  Returns the aggregate rate
+    (events of all processes / the slowest process's loop time)."""
     drv = os.path.join(HERE, "oracle", "_ref", "ref_driver")
     if not os.path.exists(drv):
         return None, "oracle/_ref/ref_driver not built"
-    with tempfile.TemporaryDirectory() as d:
+    dirs = [tempfile.mkdtemp(prefix="mgk_ref_") for _ in cfg_paths]
+    procs = [subprocess.Popen([drv, "kmc_trace", c, d, "1000000", str(n_events)], stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, text=True) for c, d in zip(cfg_paths, dirs)]
+    t_end = time.time() + timeout
+    errs = []
+    for p in procs:
         try:
-            r = subprocess.run([drv, "kmc_trace", cfg_path, d, "1000000", str(n_events)], capture_output=True, text=True,
-                               timeout=timeout)
+            _, err = p.communicate(timeout=max(1.0, t_end - time.time()))
         except subprocess.TimeoutExpired:
-            return None, "reference sample exceeded %.0f s" % timeout
-        if r.returncode != 0:
-            return None, "ref_driver failed: " + r.stderr[-300:]
+            p.kill()
+            p.communicate()
+            errs.append("reference sample exceeded %.0f s" % timeout)
+            continue
+        if p.returncode != 0:
+            errs.append("ref_driver failed: " + (err or "")[-300:])
+    if errs:
+        return None, errs[0]
+    nev, secs = 0, 0.0
+    for d in dirs:
         vals = open(os.path.join(d, "timing.txt")).read().split()
-    nev, loop_s = int(float(vals[1])), float(vals[2])
-    return {"events": nev, "seconds": loop_s, "value": nev / loop_s if loop_s > 0 else 0.0}, None
+        nev += int(float(vals[1]))
+        secs = max(secs, float(vals[2]))
+    return {"events": nev, "seconds": secs, "value": nev / secs if secs > 0 else 0.0, "processes": len(cfg_paths)}, None
 
 
 def reduce_over_ranks(dist, seconds: float, events: float, device=None):
@@ -149,15 +178,118 @@ def reduce_over_ranks(dist, seconds: float, events: float, device=None):
     return float(t.item()), float(e.item())
 
 
+def sweep_bytes(cfg):
+    """Algorithmic bytes of one sweep: per mode Q0 and the catalog read, Q
+    written; per voxel the symmetric stress inputs (strain, plastic strain,
+    lam, mu) and the softening state read."""
+    D = cfg.dim
+    S = 3 if D == 2 else 6
+    C = 6 if (D == 3 and cfg.use_3d_barriers) else 2
+    return cfg.n_voxels * (cfg.M * 8 * (2 + C) + 8 * (2 * S + 2 + 3))
+
+
+def percentile(x, q):
+    return float(np.percentile(x, q)) if len(x) else None
+
+
+def ensemble_block(G, workloads, workdir, seconds, plain_events):
+    """The 64-replica mixed ensemble in one launch for `seconds` of device
+    time, and the plain form's rate per size class (plain_events events on
+    one replica of each class, one after another)."""
+    from mgkmc_cpp_b200.workloads import ENSEMBLE
+    t0 = time.time()
+    reps = workloads.ensemble(os.path.join(workdir, "ens"), ENSEMBLE)
+    cfgs = [c for _, _, c in reps]
+    b = G.KmcBatch(cfgs)
+    t_setup = time.time() - t0
+    b.run(3)
+    b.set_time_limit(seconds)
+    ms = b.run(10 ** 9)
+    st = [b.stats(r) for r in range(len(cfgs))]
+    events = sum(x["events"] for x in st)
+    vox_iters = sum(x["ls_iters"] * c.n_voxels for x, c in zip(st, cfgs))
+    lat = np.concatenate([x["event_us"] for x in st if len(x["event_us"])]) if events else np.zeros(0)
+    classes = {}
+    for name, x in zip(ENSEMBLE, st):
+        k = classes.setdefault(name, {"replicas": 0, "events": 0, "ctas": int(x["ctas"])})
+        k["replicas"] += 1
+        k["events"] += int(x["events"])
+    b.close()
+    # plain form, replica by replica: per-class rate on the class's first replica
+    kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
+    plain_time = 0.0
+    for name, k in classes.items():
+        c = cfgs[ENSEMBLE.index(name)]
+        sim = G.from_config(c, output_dir=os.path.join(workdir, "ens_plain"))
+        sim.run_simulation(10 ** 6, c.step_size, c.driving, c.targets, c.mixed_tol_pa, 50, max_events=3, **kw)
+        sim.set_profiling(True)
+        e0 = sim.stats["thermal_events"]
+        sim.run_simulation(10 ** 6, c.step_size, c.driving, c.targets, c.mixed_tol_pa, 50, max_events=plain_events,
+                           **kw)
+        ev = sim.stats["thermal_events"] - e0
+        rate = ev / (sim.profile()["run_ms"] / 1e3) if ev else 0.0
+        k["plain_steps_per_s"] = rate
+        if rate > 0:
+            plain_time += k["events"] / rate
+        del sim
+    chosen = events / (ms / 1e3) if ms > 0 else 0.0
+    plain = events / plain_time if plain_time > 0 else None
+    return {"replicas": len(cfgs), "composition": "16x2D 64^2, 16x2D 128^2, 16x2D 512^2, 5x3D 32^3, 5x3D 48^3, "
+                                                "6x3D 96^3 (M 18 in 2D, 100 in 3D)",
+            "device_seconds": ms / 1e3, "events": int(events), "value": chosen, "unit": UNIT,
+            "ls_voxel_iterations_per_s": vox_iters / (ms / 1e3) if ms > 0 else None,
+            "plain_replica_by_replica": plain, "speedup_vs_plain": (chosen / plain) if plain else None,
+            "latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},
+            "per_class": classes, "setup_seconds": t_setup}
+
+
+def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_events=50):
+    """The serving loop on a Poisson request stream (20 jobs/s, seed 7): jobs
+    are admitted as they arrive (wall clock) and as memory allows, every
+    active job advances in shared batched launches of slice_events events,
+    finished jobs retire.  Returns throughput, per-step latency and job
+    completion latency."""
+    jobs = workloads.serve_jobs(os.path.join(workdir, "serve"), n_jobs, flips=flips, sizes=sizes)
+    srv = G.Server(slice_events=slice_events)
+    for arrival, cfg, target in jobs:
+        srv.submit(cfg, target, arrival=arrival)
+    t0 = time.perf_counter()
+    dev_ms = 0.0
+    while not srv.idle():
+        now = time.perf_counter() - t0
+        if not srv.active and srv.queue and srv.queue[0]["arrival"] > now:
+            time.sleep(min(0.05, srv.queue[0]["arrival"] - now))
+            continue
+        dev_ms += srv.step(now)
+    wall = time.perf_counter() - t0
+    done = list(srv.done.values())
+    events = sum(j["events"] for j in done)
+    comp = [j["finished"] - j["arrival"] for j in done]
+    lat = np.array(srv.step_latency_us)
+    return {"jobs": len(done), "arrivals": "Poisson 20 jobs/s, seed 7", "flips_per_job": list(flips),
+            "sizes": ["%s %d" % x for x in sizes], "slice_events": slice_events, "events": int(events),
+            "wall_seconds": wall, "device_seconds": dev_ms / 1e3, "launches": srv.launches,
+            "value": events / wall if wall > 0 else None, "unit": UNIT,
+            "step_latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},
+            "job_completion_s": {"p50": percentile(comp, 50), "p99": percentile(comp, 99)}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=1000, help="thermal events per replica in the timed region")
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--cpu-events", type=int, default=40, help="events in the bounded CPU-baseline sample")
-    ap.add_argument("--ref-events", type=int, default=150, help="events timed by --impl reference (bounded sample)")
+    ap.add_argument("--replicas", type=int, default=4)
+    ap.add_argument("--cpu-events", type=int, default=40, help="events per replica in the bounded CPU-baseline sample")
+    ap.add_argument("--ref-events", type=int, default=150, help="events per replica timed by --impl reference")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-replica ensemble block")
+    ap.add_argument("--ensemble-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-jobs", type=int, default=40, help="jobs of the serving block (0: skip)")
+    ap.add_argument("--serve-flips", type=int, nargs=2, default=[50, 500])
+    ap.add_argument("--serve-full-sizes", action="store_true",
+                    help="serve the full size set (2D 32^2..512^2, 3D 32^3, 64^3); default 2D 32^2..256^2, 3D 32^3")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -168,27 +300,37 @@ def main():
     from mgkmc_cpp_b200 import workloads
 
     workdir = tempfile.mkdtemp(prefix="mgk_bench_")
-    cfg_path, cfg = workloads.write_workload(args.workload, workdir, seed=rank)
-    base_cfg = {"workload": args.workload, "grid": [cfg.nx, cfg.ny] + ([cfg.nz] if cfg.dim == 3 else []), "M": cfg.M,
-                "modes": cfg.n_voxels * cfg.M, "temperature_K": cfg.temperature, "step": "one thermal KMC event",
-                "form": "plain (fp64, host RNG replay of the reference's draws)",
-                "l2": "working set < L2 (126 MB); no flush between steps",
-                "parallelism": "replicas" if args.gpus > 1 else "single"}
+    seeds = [args.replicas * rank + i for i in range(args.replicas)]
+    made = [workloads.write_workload(args.workload, workdir, seed=sd) for sd in seeds]
+    cfg_paths = [m[0] for m in made]
+    cfgs = [m[1] for m in made]
+    cfg = cfgs[0]
+    base_cfg = {"workload": args.workload, "replicas": args.replicas, "seeds": seeds,
+                "grid": [cfg.nx, cfg.ny] + ([cfg.nz] if cfg.dim == 3 else []), "M": cfg.M,
+                "modes_per_replica": cfg.n_voxels * cfg.M, "temperature_K": cfg.temperature,
+                "step": "one thermal KMC event of one replica", "steps_are": "thermal events per replica",
+                "form": "chosen: batched device-resident kernel, fp64, the reference's RNG stream continued on the GPU",
+                "l2": "working set < L2 (126 MB) per replica; no flush between steps",
+                "parallelism": "replicas" if args.gpus > 1 else "single GPU, %d replicas" % args.replicas}
 
     if args.impl == "reference":
         if rank != 0:
             return 0
-        res, err = run_reference(cfg_path, max(3, min(args.steps, args.ref_events)))
+        res, err = run_reference(cfg_paths, max(3, min(args.steps, args.ref_events)))
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": err}))
             return 0
-        sample = ("first %d thermal events of %s: the reference's KmcSimulation2D/3D methods driven through "
-                  "run_simulation's control flow, single-threaded by construction" % (res["events"], args.workload))
+        sample = ("first %d thermal events of each of %d replicas of %s (seeds %s), one process per replica run "
+                  "concurrently: the reference's KmcSimulation2D/3D methods driven through run_simulation's control "
+                  "flow, each single-threaded by construction" % (res["events"] // len(cfg_paths), len(cfg_paths),
+                                                                   args.workload, seeds))
         line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
-                "steps": res["events"], "warmup": 0, "ms_per_step": 1e3 * res["seconds"] / max(res["events"], 1),
+                "steps": res["events"] // len(cfg_paths), "warmup": 0,
+                "ms_per_step": 1e3 * res["seconds"] * len(cfg_paths) / max(res["events"], 1),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded lognormal modulus field)", "config": base_cfg,
-                "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+                "data": "synthetic (seeded lognormal modulus fields)", "config": base_cfg,
+                "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": len(cfg_paths), "kind": "reference",
+                                 "sample": sample},
                 "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -207,81 +349,144 @@ def main():
         tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
         dist = tdist
 
-    sim = G.from_config(cfg, output_dir=os.path.join(workdir, "out"))
-    kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
-
-    def segment(n):
-        sim.run_simulation(10 ** 6, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50, max_events=n, **kw)
-
     def barrier():
         if dist is not None:
             import torch
             torch.cuda.synchronize()
             dist.barrier()
 
-    segment(args.warmup)
-    # timed region: device-resident state, CUDA-event timing on the engine stream
-    sim.set_profiling(True)
-    st0 = sim.stats
+    # chosen form: all replicas in one device-resident launch
+    batch = G.KmcBatch(cfgs)
+    batch.run(args.warmup)
     clocks = ClockSampler(local_rank)
     clocks.start()
     barrier()
-    segment(args.steps)
+    ms = batch.run(args.steps)
     barrier()
     clk = clocks.stop()
+    st = [batch.stats(r) for r in range(len(cfgs))]
+    ev = sum(x["events"] for x in st)
+    t_chosen, ev_all = reduce_over_ranks(dist, ms / 1e3, ev, dev)
+    value = ev_all / t_chosen if t_chosen > 0 else 0.0
+    lat = np.concatenate([x["event_us"] for x in st])
+    iters = sum(x["ls_iters"] for x in st)
+    sweeps = sum(x["sweeps"] for x in st)
+    # e2e of the chosen form: the public call (its control blocks and
+    # generator states to the device, counters, generator states, selections
+    # and event times back) plus every replica's macroscopic result read back
+    barrier()
+    t0 = time.perf_counter()
+    batch.run(args.steps)
+    macros = [batch.macro(r) for r in range(len(cfgs))]
+    barrier()
+    t_e2e = time.perf_counter() - t0
+    st2 = [batch.stats(r) for r in range(len(cfgs))]
+    ev2 = sum(x["events"] for x in st2)
+    h2d = sum(x["h2d_bytes"] for x in st2)
+    d2h = sum(x["d2h_bytes"] for x in st2) + sum(m.nbytes for m in macros)
+    t_e2e, ev2_all = reduce_over_ranks(dist, t_e2e, ev2, dev)
+    e2e_value = ev2_all / t_e2e if t_e2e > 0 else 0.0
+    batch.close()
+
+    # plain form: the drop-in engine, one replica (seed of this rank's first replica)
+    sim = G.from_config(cfg, output_dir=os.path.join(workdir, "out"))
+    kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
+
+    def segment(n):
+        sim.run_simulation(10 ** 6, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50, max_events=n, **kw)
+
+    segment(args.warmup)
+    sim.set_profiling(True)
+    p0 = sim.stats
+    barrier()
+    segment(args.steps)
+    barrier()
     prof = sim.profile()
-    st1 = sim.stats
-    events = st1["thermal_events"] - st0["thermal_events"]
-    t_run, events_all = reduce_over_ranks(dist, prof["run_ms"] / 1e3, events, dev)
-    value = events_all / t_run if t_run > 0 else 0.0
-    lat = prof["event_us"]
-    # e2e: the public API call under the host clock.  Every step copies its
-    # inputs (target u2*total and the M redraw records, pinned) host->device and
-    # reads its result (rate total, selection, LS macro tensors) device->host.
+    p1 = sim.stats
+    pev = p1["thermal_events"] - p0["thermal_events"]
+    t_plain, pev_all = reduce_over_ranks(dist, prof["run_ms"] / 1e3, pev, dev)
+    plain_value = pev_all / t_plain if t_plain > 0 else 0.0
     sim.set_profiling(False)
     barrier()
     t0 = time.perf_counter()
     segment(args.steps)
     barrier()
-    t_e2e = time.perf_counter() - t0
-    st2 = sim.stats
-    t_e2e, ev_e2e = reduce_over_ranks(dist, t_e2e, st2["thermal_events"] - st1["thermal_events"], dev)
-    e2e_value = ev_e2e / t_e2e if t_e2e > 0 else 0.0
+    tp_e2e = time.perf_counter() - t0
+    p2 = sim.stats
+    tp_e2e, pev2 = reduce_over_ranks(dist, tp_e2e, p2["thermal_events"] - p1["thermal_events"], dev)
+    plain_e2e = pev2 / tp_e2e if tp_e2e > 0 else 0.0
+    del sim
+
+    ens = None
+    if not args.no_ensemble and rank == 0:
+        try:
+            ens = ensemble_block(G, workloads, workdir, args.ensemble_seconds, 20)
+        except Exception as e:  # reported, never silently dropped
+            ens = {"error": str(e)[-300:]}
+    srv = None
+    if args.serve_jobs > 0 and rank == 0:
+        sizes = workloads.SERVE_SIZES if args.serve_full_sizes else [x for x in workloads.SERVE_SIZES
+                                                                     if x in (("2d", 32), ("2d", 64), ("2d", 128),
+                                                                              ("2d", 256), ("3d", 32))]
+        try:
+            srv = serve_block(G, workloads, workdir, args.serve_jobs, tuple(args.serve_flips), sizes)
+        except Exception as e:
+            srv = {"error": str(e)[-300:]}
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return 0
     peak, peak_kind = peaks()
+    # roofline of the chosen form's kernel: algorithmic bytes of its sweeps
+    # and LS iterations over the launch's CUDA-event time
+    alg_bytes = sweeps * sweep_bytes(cfg) + iters * BYTES_LS[cfg.dim] * cfg.n_voxels
+    achieved = alg_bytes / (ms / 1e3) / 1e9 if ms > 0 else 0.0
     n_launch = max(prof["ls_launches"], 1)
     avg_ms = prof["ls_ms"] / n_launch
-    alg_bytes = BYTES_LS[cfg.dim] * cfg.n_voxels * prof["ls_iterations"] / n_launch
-    achieved = alg_bytes / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
-    C = 6 if (cfg.dim == 3 and cfg.use_3d_barriers) else 2
-    kernel_ms = {"ls_kernel": prof["ls_ms"], "sweep_kernel": prof["sweep_ms"], "select_flip_kernel": prof["select_ms"],
-                 "timed_region": prof["run_ms"]}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": int(events_all),
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_run / max(events, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lognormal modulus field)",
-            "config": dict(base_cfg, ls_iterations_per_step=prof["ls_iterations"] / max(events, 1), kernel_ms=kernel_ms,
-                           cascades=st1["cascades"] - st0["cascades"]),
-            "latency_us": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
-                           "p99": float(np.percentile(lat, 99)) if len(lat) else None},
-            "roofline": {"kernel": "ls_kernel (one persistent launch per LS solve)", "bound": "hbm",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_kind, "traffic": traffic_from_profiles(args.workload),
-                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * (1 + cfg.M * (C + 1)),
-                    "d2h_bytes_per_step": 56 + 112 + 4},
-            "gpu_launches": int(st1["launches"] - st0["launches"]),
+    ls_bytes = BYTES_LS[cfg.dim] * cfg.n_voxels * prof["ls_iterations"] / n_launch
+    ls_achieved = ls_bytes / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_chosen / max(ev, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lognormal modulus fields)",
+            "config": dict(base_cfg, ls_iterations_per_step=iters / max(ev, 1), sweeps_per_step=sweeps / max(ev, 1),
+                           ctas_per_replica=[int(x["ctas"]) for x in st],
+                           phase_ms={k[3:]: round(sum(x[k] for x in st) / len(st), 3) for k in st[0] if k.startswith("ms_")}),
+            "latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99),
+                           "what": "device time between consecutive thermal events of a replica"},
+            "ls_voxel_iterations_per_s": iters * cfg.n_voxels / (ms / 1e3) if ms > 0 else None,
+            "roofline": {"kernel": "batch_kernel (one persistent launch: every replica's sweeps, selections, flips, "
+                                   "redraws and LS solves)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": ms},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / max(ev2, 1),
+                    "d2h_bytes_per_step": d2h / max(ev2, 1)},
+            "gpu_launches": 1,
+            "plain": {"value": plain_value, "unit": UNIT, "what": "drop-in form (mgk_kmc_run), replica by replica",
+                      "chosen_speedup": value / plain_value if plain_value > 0 else None,
+                      "latency_us": {"p50": percentile(prof["event_us"], 50), "p99": percentile(prof["event_us"], 99)},
+                      "e2e": {"value": plain_e2e, "unit": UNIT,
+                              "h2d_bytes_per_step": 8 * (1 + cfg.M * ((6 if (cfg.dim == 3 and cfg.use_3d_barriers) else 2) + 1)),
+                              "d2h_bytes_per_step": 56 + 112 + 4},
+                      "gpu_launches": int(p1["launches"] - p0["launches"]),
+                      "roofline": {"kernel": "ls_kernel (one persistent launch per LS solve)", "bound": "hbm",
+                                   "achieved": ls_achieved, "peak": peak, "unit": "GB/s", "frac": ls_achieved / peak,
+                                   "traffic": traffic_from_profiles(args.workload), "alg_bytes_per_launch": ls_bytes,
+                                   "avg_launch_ms": avg_ms}},
             "clocks": clk}
+    if ens is not None:
+        line["ensemble"] = ens
+    if srv is not None:
+        line["serving"] = srv
     if args.gpus == 1:
-        res, err = run_reference(cfg_path, args.cpu_events)
+        res, err = run_reference(cfg_paths, args.cpu_events)
         if res is not None:
-            line["cpu_baseline"] = {"value": res["value"], "unit": UNIT, "cores": 1, "kind": "reference",
-                                    "sample": "first %d thermal events of the same workload, reference code "
-                                              "(oracle/_ref/ref_driver), setup excluded" % res["events"]}
+            line["cpu_baseline"] = {"value": res["value"], "unit": UNIT, "cores": len(cfg_paths), "kind": "reference",
+                                    "sample": "first %d thermal events of each replica of the same workload, one "
+                                              "reference process (oracle/_ref/ref_driver) per replica run "
+                                              "concurrently, setup excluded" % args.cpu_events}
         else:
-            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": err}
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": len(cfg_paths), "kind": "reference",
+                                    "sample": err}
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

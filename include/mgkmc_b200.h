@@ -41,6 +41,9 @@ typedef enum {
 MGK_API const char* mgk_last_error(void);
 MGK_API int mgk_version(void);
 MGK_API int mgk_device_count(void);
+/* Free and total memory of the current device, in bytes (admission control of
+ * a request loop). */
+MGK_API mgk_status mgk_device_memory(unsigned long long* free_bytes, unsigned long long* total_bytes);
 
 /* ---------------------------------------------------------------- LS solver
  * Replaces spectral_solver_2d (linear_elastic_solver.hpp:146-160) and
@@ -155,6 +158,38 @@ MGK_API mgk_status mgk_kmc_get_field(mgk_kmc* h, int field, double* dst, long lo
 MGK_API mgk_status mgk_kmc_get_macro(mgk_kmc* h, double* out, int n);
 MGK_API void mgk_kmc_destroy(mgk_kmc* h);
 
+/* ---------------------------------------------------------------- linear-elastic simulation
+ * Replaces main.cpp's simulation_type "linear_elastic" branch
+ * (main.cpp:418-869): the macroscopic target (eps_target on the driving
+ * component drive_i, drive_j; zero strain on the other components; the mixed
+ * stress targets, in Pa, on their components) is applied proportionally in
+ * n_steps = round(eps_target / step_size) steps, s = 0 .. n_steps; each step
+ * runs up to max_iter_macro (the reference: 20) warm-started LS solves
+ * (max_iter_ls 200, tol_ls 1e-6 there), correcting the stress-controlled
+ * strain components by (err - nu_avg tr(err) I) / E_avg until every stress
+ * error is below mixed_tol (Pa).  Writes the reference's summary and global
+ * logs and VTU files into output_dir (NULL: no files).  macro_out (nullable)
+ * gets (n_steps + 1) x 2 x D x D values: per step eps_macro then sig_macro,
+ * row-major; ls_iters_out (nullable) the LS iterations of the whole run. */
+typedef struct {
+    int dim, nx, ny, nz, plane_stress;
+    double pixel;
+    double eps_target, step_size;
+    int drive_i, drive_j;
+    int n_targets;
+    int target_i[9], target_j[9];
+    double target_v[9];
+    double mixed_tol;
+    int max_iter_macro, max_iter_ls;
+    double tol_ls;
+    const char* output_dir;
+    const char* summary_filename;
+    int enable_summary_log, enable_global_log, enable_console;
+    const char* vtk_interval; /* "none", "last", "current" or a step interval */
+} mgk_le_params;
+MGK_API mgk_status mgk_le_run(const mgk_le_params* p, const double* E, const double* nu, double* macro_out,
+                              int* ls_iters_out);
+
 /* ---------------------------------------------------------------- batched, device-resident KMC
  * No counterpart in the reference (single replica, single thread there).  n
  * independent simulations, each constructed exactly like mgk_kmc_create, run
@@ -167,12 +202,13 @@ MGK_API void mgk_kmc_destroy(mgk_kmc* h);
  * (<= 0: until its n_global_steps elastic steps are done); rp holds n entries
  * (log and VTU fields are ignored: device-resident runs write no files);
  * elapsed_ms gets the kernel's CUDA-event time.  mgk_batch_stats fills
- * out[0..15] = {events, cascades, cascade flips, LS solves, LS iterations,
+ * out[0..18] = {events, cascades, cascade flips, LS solves, LS iterations,
  * elastic steps, selection fallbacks, smallest selection margin, terminated
  * (1 instability sequence limit, 2 time limit), CTAs of the replica, then the
  * replica's device time in ms spent in: sweeps, decisions (selection, flip,
  * redraw), event LS solves, cascade collection and flips, cascade LS solves,
- * interval ends (mixed-BC loop)} and
+ * interval ends (mixed-BC loop), then the number of sweeps and the bytes the
+ * run call copied host-to-device and device-to-host for the replica} and
  * copies the flat mode index of each thermal event of the last run into sel
  * (up to sel_cap; *sel_len gets the count).  A run stops every replica whose
  * run call has lasted longer than the time limit (default 60 s, set with
@@ -181,10 +217,22 @@ MGK_API void mgk_kmc_destroy(mgk_kmc* h);
 typedef struct mgk_batch mgk_batch;
 MGK_API mgk_status mgk_batch_create(mgk_batch** out, int n, const mgk_kmc_params* params, const double* const* E,
                                     const double* const* nu);
+/* A batch over n existing simulations (mgk_kmc_create), not owned: they
+ * must outlive the batch, and mgk_kmc_get_field / get_macro read them after
+ * a run.  A simulation may join different batches over its life (one running
+ * batch at a time); its interval clock and random stream carry over, which is
+ * how a request loop admits and retires jobs between launches. */
+MGK_API mgk_status mgk_batch_create_from(mgk_batch** out, int n, mgk_kmc* const* sims);
+/* rp[r].max_events > 0 sets replica r's own event budget for the call. */
 MGK_API mgk_status mgk_batch_run(mgk_batch* h, const mgk_run_params* rp, long long max_events, double* elapsed_ms);
 MGK_API mgk_status mgk_batch_stats(mgk_batch* h, int replica, double* out, int* sel, long long sel_cap, long long* sel_len);
 MGK_API mgk_status mgk_batch_get_field(mgk_batch* h, int replica, int field, double* dst, long long* count);
 MGK_API mgk_status mgk_batch_get_macro(mgk_batch* h, int replica, double* out, int n);
+/* Per-step latency of the last run: for each logged thermal event of the
+ * replica (up to 65536), the device time in microseconds since its previous
+ * event (the first: since the run's first decision).  Copies up to cap values
+ * into us; *len gets the count.  No counterpart in the reference. */
+MGK_API mgk_status mgk_batch_event_times(mgk_batch* h, int replica, double* us, long long cap, long long* len);
 MGK_API mgk_status mgk_batch_set_time_limit(mgk_batch* h, double seconds);
 MGK_API void mgk_batch_destroy(mgk_batch* h);
 

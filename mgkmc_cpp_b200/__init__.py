@@ -27,7 +27,8 @@ from . import _lib
 from ._lib import MgkError
 
 __all__ = ["BarrierGenerator", "LsSolver", "spectral_solver_2d", "spectral_solver_3d", "KmcSimulation2D",
-           "KmcSimulation3D", "KmcBatch", "from_config", "MgkError"]
+           "KmcSimulation3D", "KmcBatch", "Server", "from_config", "linear_elastic_run", "run_config",
+           "MgkError"]
 
 _BAR = {"gaussian": 0, "rayleigh": 1, "modified_rayleigh": 2, "modified_rayleigh_with_exponential": 3}
 
@@ -318,9 +319,173 @@ def from_config(cfg, output_dir: Optional[str] = None):
               redraw_directions=cfg.redraw_directions, redraw_barriers=cfg.redraw_barriers, seed=cfg.seed,
               ls_tol=cfg.ls_tol, ls_max_iter=cfg.ls_max_iter)
     if cfg.dim == 3:
-        return KmcSimulation3D(cfg.nx, cfg.ny, cfg.nz, cfg.M, cfg.gamma0, cfg.E, cfg.nu,
-                               use_3d_barriers=cfg.use_3d_barriers, **kw)
-    return KmcSimulation2D(cfg.nx, cfg.ny, cfg.M, cfg.gamma0, cfg.E, cfg.nu, plane_mode=cfg.plane_mode, **kw)
+        sim = KmcSimulation3D(cfg.nx, cfg.ny, cfg.nz, cfg.M, cfg.gamma0, cfg.E, cfg.nu,
+                              use_3d_barriers=cfg.use_3d_barriers, **kw)
+    else:
+        sim = KmcSimulation2D(cfg.nx, cfg.ny, cfg.M, cfg.gamma0, cfg.E, cfg.nu, plane_mode=cfg.plane_mode, **kw)
+    sim._cfg = cfg
+    return sim
+
+
+def linear_elastic_run(cfg, output_dir: Optional[str] = None, write_files: bool = True, max_iter_macro: int = 20,
+                       max_iter_ls: int = 200, tol_ls: float = 1e-6):
+    """simulation_type "linear_elastic" of main.cpp:418-869 on the GPU: the
+    proportional-loading schedule with the mixed stress/strain loop, its logs
+    and VTU files (in output_dir, default the config's output.directory).
+    Returns (eps_macro, sig_macro, ls_iterations): arrays of shape
+    (n_steps + 1, D, D)."""
+    L = _lib.lib()
+    _lib.require_device()
+    D = cfg.dim
+    p = _lib.LeParamsC()
+    p.dim, p.nx, p.ny, p.nz = D, cfg.nx, cfg.ny, cfg.nz if D == 3 else 1
+    p.plane_stress = 1 if cfg.plane_mode == "plane_stress" else 0
+    p.pixel, p.eps_target, p.step_size = float(cfg.pixel), float(cfg.eps_target), float(cfg.step_size)
+    p.drive_i, p.drive_j = cfg.driving
+    tg = sorted(cfg.targets.items())
+    p.n_targets = len(tg)
+    for k, ((i, j), v) in enumerate(tg):
+        p.target_i[k], p.target_j[k], p.target_v[k] = i, j, v
+    p.mixed_tol = float(cfg.mixed_tol_pa)
+    p.max_iter_macro, p.max_iter_ls, p.tol_ls = int(max_iter_macro), int(max_iter_ls), float(tol_ls)
+    out = output_dir or cfg.output_directory
+    if write_files:
+        os.makedirs(out, exist_ok=True)
+        p.output_dir = out.encode()
+    else:
+        p.output_dir = None
+    p.summary_filename = cfg.summary_filename.encode()
+    p.enable_summary_log, p.enable_global_log = int(cfg.enable_summary_log), int(cfg.enable_global_log)
+    p.enable_console = int(cfg.enable_console)
+    p.vtk_interval = str(cfg.vtk_interval).encode()
+    n_steps = cfg.n_steps
+    E = np.ascontiguousarray(cfg.E, dtype=np.float64).reshape(-1)
+    nu = np.ascontiguousarray(cfg.nu, dtype=np.float64).reshape(-1)
+    mac = np.zeros((n_steps + 1) * 2 * D * D)
+    it = _lib.C.c_int(0)
+    _lib.check(L.mgk_le_run(_lib.C.byref(p), _lib.dptr(E), _lib.dptr(nu), _lib.dptr(mac), _lib.C.byref(it)))
+    mac = mac.reshape(n_steps + 1, 2, D, D)
+    return mac[:, 0], mac[:, 1], int(it.value)
+
+
+def run_config(path_or_cfg, output_dir: Optional[str] = None):
+    """What the reference executable does with a config file (main.cpp:25-416):
+    a KMC run (run_simulation with the config's schedule) or the
+    linear-elastic simulation."""
+    from .config import SimConfig
+    cfg = path_or_cfg if not isinstance(path_or_cfg, str) else SimConfig.from_yaml(path_or_cfg)
+    out = output_dir or cfg.output_directory
+    os.makedirs(out, exist_ok=True)
+    if cfg.simulation_type == "linear_elastic":
+        return linear_elastic_run(cfg, out)
+    sim = from_config(cfg, output_dir=out)
+    sim.run_simulation(cfg.n_steps, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50,
+                       enable_console_log=cfg.enable_console, summary_filename=cfg.summary_filename,
+                       enable_summary_log=cfg.enable_summary_log, enable_global_log=cfg.enable_global_log,
+                       vtk_interval=cfg.vtk_interval, vtk_elastic_only=cfg.vtk_elastic_only,
+                       max_kmc_steps_pct=cfg.max_kmc_steps_pct)
+    return sim
+
+
+def device_memory():
+    """(free, total) bytes of the current device."""
+    f, t = _lib.C.c_ulonglong(0), _lib.C.c_ulonglong(0)
+    _lib.check(_lib.lib().mgk_device_memory(_lib.C.byref(f), _lib.C.byref(t)))
+    return int(f.value), int(t.value)
+
+
+def job_device_bytes(cfg) -> int:
+    """Device memory of one simulation: per mode Q0, Q and the catalog; per
+    voxel the strain, plastic strain, stress inputs, spectrum, softening and
+    KMC bookkeeping (FP64)."""
+    D = cfg.dim
+    S = 3 if D == 2 else 6
+    C = 6 if (D == 3 and cfg.use_3d_barriers) else 2
+    N = cfg.n_voxels
+    return int(N * cfg.M * 8 * (2 + C) + N * 8 * (4 * S + 2 + 2 + 2 * S + 2 + 1 + C) + (64 << 10))
+
+
+class Server:
+    """Continuous batching of KMC jobs on one GPU (the serving loop).
+
+    ``submit(cfg, flips)`` queues a job (a simulation that must reach
+    ``flips`` thermal events).  Each ``step()`` admits queued jobs, in
+    arrival order, while the active set is below ``max_active`` and the job's
+    device memory (``job_device_bytes``) fits: the active jobs' memory plus
+    the new job's stays within ``hbm_budget`` (default: the device's free
+    memory when the server starts, less ``reserve_bytes``), and the device
+    has that much free right now.  Admitted jobs keep their fields and random
+    stream resident on the device.  The step then advances every active job
+    by up to ``slice_events`` events in one batched launch and retires the
+    jobs that reached their target.  A job's trajectory does not depend on
+    what shares its launches: its random stream and interval clock are its
+    own."""
+
+    def __init__(self, max_active=64, slice_events=50, reserve_bytes=8 << 30, hbm_budget=None, time_limit=60.0):
+        self.max_active, self.slice_events, self.reserve = int(max_active), int(slice_events), int(reserve_bytes)
+        self.budget = int(hbm_budget) if hbm_budget is not None else device_memory()[0] - self.reserve
+        self.committed = 0
+        self.time_limit = float(time_limit)
+        self.queue, self.active, self.done = [], [], {}
+        self._next = 0
+        self.launches = 0
+        self.step_latency_us = []
+
+    def submit(self, cfg, flips: int, arrival: float = 0.0) -> int:
+        jid = self._next
+        self._next += 1
+        self.queue.append({"id": jid, "cfg": cfg, "target": int(flips), "events": 0, "selected": [],
+                           "arrival": float(arrival), "admitted": None, "finished": None, "latency_us": []})
+        return jid
+
+    def _admit(self, now: float):
+        while self.queue and len(self.active) < self.max_active and self.queue[0]["arrival"] <= now:
+            job = self.queue[0]
+            need = job_device_bytes(job["cfg"])
+            if self.committed + need > self.budget or need > device_memory()[0]:
+                break
+            self.queue.pop(0)
+            job["sim"] = from_config(job["cfg"], output_dir=None)
+            job["bytes"] = need
+            self.committed += need
+            job["admitted"] = now
+            self.active.append(job)
+
+    def step(self, now: float = 0.0) -> float:
+        """One slice; returns the launch's device milliseconds (0 if idle)."""
+        self._admit(now)
+        if not self.active:
+            return 0.0
+        b = KmcBatch(sims=[j["sim"] for j in self.active])
+        b.cfgs = [j["cfg"] for j in self.active]
+        b.set_time_limit(self.time_limit)
+        ms = b.run(self.slice_events,
+                   budgets=[min(self.slice_events, j["target"] - j["events"]) for j in self.active])
+        self.launches += 1
+        keep = []
+        for r, job in enumerate(self.active):
+            st = b.stats(r)
+            job["events"] += int(st["events"])
+            job["selected"].append(st["selected"])
+            job["latency_us"].extend(st["event_us"].tolist())
+            self.step_latency_us.extend(st["event_us"].tolist())
+            if job["events"] >= job["target"] or st["terminated"]:
+                job["finished"] = now
+                job["selected"] = np.concatenate(job["selected"]) if job["selected"] else np.zeros(0, np.int64)
+                job["eps_field"] = job["sim"].eps_field
+                job["macro"] = job["sim"].macro()
+                job["sim"].close()
+                del job["sim"]
+                self.committed -= job["bytes"]
+                self.done[job["id"]] = job
+            else:
+                keep.append(job)
+        b.close()
+        self.active = keep
+        return ms
+
+    def idle(self) -> bool:
+        return not self.queue and not self.active
 
 
 def kmc_params_from_config(cfg) -> "_lib.KmcParamsC":
@@ -373,9 +538,22 @@ class KmcBatch:
     no host round trip per event; the reference's random stream continued on
     the device.  ``configs`` is a list of SimConfig."""
 
-    def __init__(self, configs):
+    def __init__(self, configs=None, sims=None):
+        """``configs``: SimConfigs, one new simulation each (owned).  ``sims``:
+        existing simulations (KmcSimulation2D/3D from ``from_config``) to
+        advance in place; they keep their state after the batch is gone."""
         L = _lib.lib()
         _lib.require_device()
+        if sims is not None:
+            self.sims = list(sims)
+            self.cfgs = [getattr(x, "_cfg", None) for x in self.sims]
+            n = len(self.sims)
+            hs = (_lib.C.c_void_p * n)(*[x._h.value for x in self.sims])
+            h = _lib.C.c_void_p()
+            _lib.check(L.mgk_batch_create_from(_lib.C.byref(h), n, hs))
+            self._h = h
+            return
+        self.sims = None
         self.cfgs = list(configs)
         n = len(self.cfgs)
         self._params = (_lib.KmcParamsC * n)(*[kmc_params_from_config(c) for c in self.cfgs])
@@ -392,12 +570,16 @@ class KmcBatch:
         """Wall-time bound of one run call (default 60 s)."""
         _lib.check(_lib.lib().mgk_batch_set_time_limit(self._h, float(seconds)))
 
-    def run(self, max_events: int, n_global_steps=10 ** 6, max_cascade_batches=0) -> float:
-        """Advance every replica by up to max_events thermal events; returns
+    def run(self, max_events: int, n_global_steps=10 ** 6, max_cascade_batches=0, budgets=None) -> float:
+        """Advance every replica by up to max_events thermal events (budgets:
+        one count per replica instead); returns
         the kernel time in milliseconds.  A run that reaches the time limit
         returns normally with ``self.time_limited`` set."""
         n = len(self.cfgs)
         rps = (_lib.RunParamsC * n)(*[run_params_from_config(c, n_global_steps, max_cascade_batches) for c in self.cfgs])
+        if budgets is not None:
+            for r, b in enumerate(budgets):
+                rps[r].max_events = int(b)
         ms = np.zeros(1)
         st = _lib.lib().mgk_batch_run(self._h, rps, int(max_events), _lib.dptr(ms))
         self.time_limited = st == 9
@@ -406,16 +588,19 @@ class KmcBatch:
         return float(ms[0])
 
     def stats(self, r: int) -> dict:
-        out = np.zeros(16)
+        out = np.zeros(19)
         cap = 1 << 16
         sel = (_lib.C.c_int * cap)()
         ln = _lib.C.c_longlong(0)
         _lib.check(_lib.lib().mgk_batch_stats(self._h, r, _lib.dptr(out), sel, cap, _lib.C.byref(ln)))
         keys = ["events", "cascades", "cascade_flips", "ls_solves", "ls_iters", "elastic_steps", "fallbacks",
                 "min_margin", "terminated", "ctas", "ms_sweep", "ms_decide", "ms_event_solve", "ms_cascade_flips",
-                "ms_cascade_solve", "ms_interval_end"]
+                "ms_cascade_solve", "ms_interval_end", "sweeps", "h2d_bytes", "d2h_bytes"]
         d = {k: float(v) for k, v in zip(keys, out)}
         d["selected"] = np.array(sel[:min(ln.value, cap)], dtype=np.int64)
+        us = np.zeros(cap)
+        _lib.check(_lib.lib().mgk_batch_event_times(self._h, r, _lib.dptr(us), cap, _lib.C.byref(ln)))
+        d["event_us"] = us[:min(ln.value, cap)].copy()
         return d
 
     def field(self, r: int, name: str) -> np.ndarray:

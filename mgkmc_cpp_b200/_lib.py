@@ -18,7 +18,8 @@ STATUS = {0: "MGK_OK", 1: "MGK_LS_NOT_CONVERGED", 2: "MGK_BAD_SHAPE", 3: "MGK_OO
 EXPORTS = ["mgk_last_error", "mgk_version", "mgk_device_count", "mgk_ls_create", "mgk_ls_solve", "mgk_ls_destroy",
            "mgk_kmc_create", "mgk_kmc_run", "mgk_kmc_elastic_run", "mgk_kmc_get_field", "mgk_kmc_get_macro",
            "mgk_kmc_destroy", "mgk_kmc_set_profiling", "mgk_kmc_get_profile", "mgk_batch_create", "mgk_batch_run",
-           "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro", "mgk_batch_set_time_limit",
+           "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro", "mgk_batch_set_time_limit", "mgk_batch_event_times", "mgk_le_run",
+           "mgk_batch_create_from", "mgk_device_memory",
            "mgk_batch_destroy"]
 
 
@@ -41,6 +42,16 @@ class KmcParamsC(C.Structure):
                 ("redraw_barriers", C.c_int), ("use_3d_barriers", C.c_int), ("fast_patching", C.c_int),
                 ("patch_radius", C.c_int), ("sync_interval", C.c_int), ("ls_tol", C.c_double),
                 ("ls_max_iter", C.c_int)]
+
+
+class LeParamsC(C.Structure):
+    _fields_ = [("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("plane_stress", C.c_int),
+                ("pixel", C.c_double), ("eps_target", C.c_double), ("step_size", C.c_double), ("drive_i", C.c_int),
+                ("drive_j", C.c_int), ("n_targets", C.c_int), ("target_i", C.c_int * 9), ("target_j", C.c_int * 9),
+                ("target_v", C.c_double * 9), ("mixed_tol", C.c_double), ("max_iter_macro", C.c_int),
+                ("max_iter_ls", C.c_int), ("tol_ls", C.c_double), ("output_dir", C.c_char_p),
+                ("summary_filename", C.c_char_p), ("enable_summary_log", C.c_int), ("enable_global_log", C.c_int),
+                ("enable_console", C.c_int), ("vtk_interval", C.c_char_p)]
 
 
 class RunParamsC(C.Structure):
@@ -86,6 +97,10 @@ def lib():
     L.mgk_batch_get_field.argtypes = [vp, C.c_int, C.c_int, dp, C.POINTER(C.c_longlong)]
     L.mgk_batch_get_macro.argtypes = [vp, C.c_int, dp, C.c_int]
     L.mgk_batch_set_time_limit.argtypes = [vp, C.c_double]
+    L.mgk_batch_create_from.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
+    L.mgk_device_memory.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]
+    L.mgk_le_run.argtypes = [C.POINTER(LeParamsC), dp, dp, dp, C.POINTER(C.c_int)]
+    L.mgk_batch_event_times.argtypes = [vp, C.c_int, dp, C.c_longlong, C.POINTER(C.c_longlong)]
     L.mgk_batch_destroy.argtypes = [vp]
     L.mgk_batch_destroy.restype = None
     L.mgk_kmc_destroy.argtypes = [vp]
@@ -93,7 +108,8 @@ def lib():
     for fn in ("mgk_ls_create", "mgk_ls_solve", "mgk_kmc_create", "mgk_kmc_run", "mgk_kmc_elastic_run",
                "mgk_kmc_get_field", "mgk_kmc_get_macro", "mgk_kmc_set_profiling", "mgk_kmc_get_profile",
                "mgk_batch_create", "mgk_batch_run", "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro",
-               "mgk_batch_set_time_limit"):
+               "mgk_batch_set_time_limit", "mgk_batch_event_times", "mgk_le_run",
+               "mgk_batch_create_from", "mgk_device_memory"):
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L

@@ -15,7 +15,9 @@
 // initial draws is handed to the device and continued by one thread with the
 // reference's distributions (mt_device.cuh), so the draws follow the
 // reference's stream; only device log/exp may differ from glibc by an ulp.
+#include <atomic>
 #include <cmath>
+#include <thread>
 #include <cstring>
 #include <limits>
 #include <sstream>
@@ -30,11 +32,7 @@ namespace mgk {
 
 enum : int { ACT_EVENT = 1, ACT_CASCADE = 2, ACT_END = 3, ACT_STOP = 4 };
 
-MGK_DEV unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+
 
 struct BatchCtl {
     double time, remaining, dt_step, strain_rate;
@@ -52,7 +50,7 @@ struct BatchCtl {
     int cascade_active, cascade_batches, mixed_it, ccount;
     long long cascade_limit;
     long long max_events, events_done;
-    long long events_total, cascades, cascade_flips, ls_solves, ls_iters, elastic_steps, fallbacks;
+    long long events_total, cascades, cascade_flips, ls_solves, ls_iters, elastic_steps, fallbacks, sweeps;
     int sel_log_len, sel_log_cap;
     unsigned long long t_start_ns, limit_ns;  // device clock at the first decision; 0: unset
     unsigned long long ph_ns[6];              // sweep, decide, event solve, cascade flips, cascade solve, interval end
@@ -78,6 +76,7 @@ struct BatchRep {
     rng::Mt* mt;
     BatchCtl* ctl;
     int* sel_log;
+    unsigned long long* ev_ns;  // device clock at the end of each logged thermal event
 };
 
 namespace {
@@ -152,23 +151,37 @@ MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
     dd* ts = R.tile_sum + (long)rank * R.tile_cap;
     dd acc = {0.0, 0.0};
     int unst = 0, last = -1;
-    for (long t = wid; t < ntile; t += nw) {
-        const long i = m0 + (t << 5) + lane;
-        dd r = {0.0, 0.0};
-        if (i < m1) {
-            const int v = (int)(i / R.s.M);
-            const double q = mode_Q<D, C>(R.s, R.p, v, i, time);
-            R.s.Q[i] = q;
-            bool inc;
-            r.hi = rate_of(R.p, q, &inc);
-            if (inc) last = (int)i;
-            if (q < R.p.threshold) ++unst;
+    // four tiles per warp and pass: independent exp / reduction chains in
+    // flight (one CTA per SM leaves only 8 warps to hide latency)
+    constexpr int U = 4;
+    for (long tb = wid; tb < ntile; tb += (long)nw * U) {
+        dd r[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const long t = tb + (long)k * nw;
+            const long i = m0 + (t << 5) + lane;
+            r[k] = dd{0.0, 0.0};
+            if (t < ntile && i < m1) {
+                const int v = (int)(i / R.s.M);
+                const double q = mode_Q<D, C>(R.s, R.p, v, i, time);
+                R.s.Q[i] = q;
+                bool inc;
+                r[k].hi = rate_of(R.p, q, &inc);
+                if (inc) last = max(last, (int)i);
+                if (q < R.p.threshold) ++unst;
+            }
         }
-        r = warp_dd_sum(r);
-        if (lane == 0) {
-            ts[t] = r;
-            acc = dd_add(acc, r);
-        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) r[k] = warp_dd_sum(r[k]);
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const long t = tb + (long)k * nw;
+                if (t < ntile) {
+                    ts[t] = r[k];
+                    acc = dd_add(acc, r[k]);
+                }
+            }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -646,6 +659,79 @@ MGK_DEV void cta_sort(double* keys, int* modes, int n, unsigned char* smem, size
     __syncthreads();
 }
 
+// Sort of (keys, modes)[0..n) by key_less with every CTA of the group, for
+// lists too long for one CTA's shared memory: a bitonic network over npow2
+// entries (padded with +inf); strides whose pairs span more than one
+// tile of `tile` entries run in global memory with a group barrier after
+// each, the smaller strides of each merge size inside shared memory tile by
+// tile.  keys and modes hold npow2 entries.  Returns false when a barrier
+// wait gave up.
+MGK_DEV bool group_sort(double* keys, int* modes, int n, int npow2, int tile, int rank, int ncta, const GridBar& gb,
+                        unsigned char* smem) {
+    const long gtid = (long)rank * blockDim.x + threadIdx.x, gthreads = (long)ncta * blockDim.x;
+    for (long i = n + gtid; i < npow2; i += gthreads) {
+        keys[i] = INFINITY;
+        modes[i] = 0x7fffffff;
+    }
+    if (!grid_sync(gb)) return false;
+    double* k = reinterpret_cast<double*>(smem);
+    int* m = reinterpret_cast<int*>(smem + (size_t)tile * 8);
+    for (int size = 2; size <= npow2; size <<= 1) {
+        int stride = size >> 1;
+        for (; 2 * stride > tile; stride >>= 1) {
+            for (long i = gtid; i < npow2; i += gthreads) {
+                const long j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const bool sw = up ? key_less(keys[j], modes[j], keys[i], modes[i])
+                                       : key_less(keys[i], modes[i], keys[j], modes[j]);
+                    if (sw) {
+                        const double tk = keys[i];
+                        keys[i] = keys[j];
+                        keys[j] = tk;
+                        const int tm = modes[i];
+                        modes[i] = modes[j];
+                        modes[j] = tm;
+                    }
+                }
+            }
+            if (!grid_sync(gb)) return false;
+        }
+        for (long t0 = (long)rank * tile; t0 < npow2; t0 += (long)ncta * tile) {
+            for (int i = threadIdx.x; i < tile; i += blockDim.x) {
+                k[i] = keys[t0 + i];
+                m[i] = modes[t0 + i];
+            }
+            __syncthreads();
+            for (int st = stride; st > 0; st >>= 1) {
+                for (int i = threadIdx.x; i < tile; i += blockDim.x) {
+                    const int j = i ^ st;
+                    if (j > i) {
+                        const bool up = ((t0 + i) & size) == 0;
+                        const bool sw = up ? key_less(k[j], m[j], k[i], m[i]) : key_less(k[i], m[i], k[j], m[j]);
+                        if (sw) {
+                            const double tk = k[i];
+                            k[i] = k[j];
+                            k[j] = tk;
+                            const int tm = m[i];
+                            m[i] = m[j];
+                            m[j] = tm;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            for (int i = threadIdx.x; i < tile; i += blockDim.x) {
+                keys[t0 + i] = k[i];
+                modes[t0 + i] = m[i];
+            }
+            __syncthreads();
+        }
+        if (!grid_sync(gb)) return false;
+    }
+    return true;
+}
+
 template <int D, int C>
 MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem_bytes) {
     __shared__ LsArgs s_ls;
@@ -684,6 +770,7 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
         if (vld(&c->done)) break;
         sweep_chunk<D, C>(R, rank, c->time);
         if (!grid_sync(gb)) break;
+        if (timer) c->sweeps++;
         phase(0);
         if (rank == 0) decide<D, C>(R, &s_ring, &s_mt, smem);
         if (!grid_sync(gb)) break;
@@ -694,6 +781,7 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
             if (!group_solve<D>(R, rank, gb, smem, &s_ls)) break;
             phase(2);
             if (rank == 0 && threadIdx.x == 0) {
+                if (c->events_done < c->sel_log_cap) R.ev_ns[c->events_done] = global_ns();
                 c->events_done++;
                 c->events_total++;
                 if (c->seq_instab > c->max_seq) {
@@ -722,9 +810,22 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
                 }
             }
             if (!grid_sync(gb)) break;
+            {
+                // long lists: sorted by the whole group; short ones by rank 0 below
+                const int n = vld(&c->ccount);
+                int npow2 = 1;
+                while (npow2 < n) npow2 <<= 1;
+                if ((size_t)npow2 * 12 > smem_bytes) {
+                    int tile = 1;
+                    while ((size_t)tile * 2 * 12 <= smem_bytes && tile * 2 <= npow2) tile <<= 1;
+                    if (!group_sort(R.ckeys, R.cmodes, n, npow2, tile, rank, R.ncta, gb, smem)) break;
+                }
+            }
             if (rank == 0) {
                 const int n = vld(&c->ccount);
-                cta_sort(R.ckeys, R.cmodes, n, smem, smem_bytes);
+                int npow2 = 1;
+                while (npow2 < n) npow2 <<= 1;
+                if ((size_t)npow2 * 12 <= smem_bytes) cta_sort(R.ckeys, R.cmodes, n, smem, smem_bytes);
                 if (threadIdx.x == 0)
                     for (int f = 0; f < n; ++f) apply_flip<D, C>(R.s, R.p, R.cmodes[f], c->time, nullptr);
                 __syncthreads();
@@ -843,7 +944,46 @@ static size_t replan_ls(LsArgs& a, int D, int ncta, size_t half_budget) {
 
 BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* const* E, const double* const* nu) {
     if (n < 1) throw std::invalid_argument("empty batch");
-    for (int r = 0; r < n; ++r) eng_.emplace_back(new KmcEngine(params[r], E[r], nu[r]));
+    // replicas are built concurrently: each one's initial catalog and barrier
+    // draws run on the host (the reference's std::mt19937 stream, sequential
+    // within a replica), which dominates set-up for large grids
+    owned_eng_.resize(n);
+    {
+        int dev0 = 0;
+        cudaGetDevice(&dev0);
+        std::vector<std::string> errs(n);
+        std::atomic<int> next{0};
+        auto work = [&]() {
+            cudaSetDevice(dev0);
+            for (int r = next++; r < n; r = next++) {
+                try {
+                    owned_eng_[r].reset(new KmcEngine(params[r], E[r], nu[r]));
+                } catch (const std::exception& ex) {
+                    errs[r] = ex.what();
+                }
+            }
+        };
+        const int nt = std::max(1, std::min(n, (int)std::max(1u, std::thread::hardware_concurrency())));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        for (int r = 0; r < n; ++r)
+            if (!errs[r].empty()) throw std::runtime_error("replica " + std::to_string(r) + ": " + errs[r]);
+    }
+    for (auto& e : owned_eng_) eng_.push_back(e.get());
+    init();
+}
+
+BatchEngine::BatchEngine(const std::vector<KmcEngine*>& sims) : eng_(sims) {
+    if (eng_.empty()) throw std::invalid_argument("empty batch");
+    for (KmcEngine* e : eng_)
+        if (!e) throw std::invalid_argument("null simulation");
+    init();
+}
+
+void BatchEngine::init() {
+    const int n = (int)eng_.size();
     BCK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -855,28 +995,37 @@ BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* cons
     const size_t half_budget = 92 * 1024;
     const int budget = per_sm * nsm;
     if (n > budget) throw std::invalid_argument("more replicas than co-resident CTAs");
-    // CTA groups sized by work per event (modes + LS voxels), within the budget
+    // CTA groups: every replica gets one CTA, then each further CTA goes to
+    // the replica whose event rate it raises most, by the model
+    // t_event(c) = kSecPerWork * work / c + kSecPerEvent (work = modes swept +
+    // 24 x LS voxels; the constants are fitted to measured 64^2 runs on one
+    // and nine CTAs).  This maximises the batch's total steps/s: small grids,
+    // whose events are latency-bound, gain most from extra CTAs; the largest
+    // grids still advance on the CTAs their share of the model gives them.
+    constexpr double kSecPerWork = 12.7e-9, kSecPerEvent = 160e-6;
     std::vector<double> work(n);
-    double tot = 0.0;
+    std::vector<int> lim(n);
     for (int r = 0; r < n; ++r) {
         work[r] = (double)eng_[r]->NM_ + 24.0 * eng_[r]->N_;
-        tot += work[r];
+        lim[r] = std::max(1, std::min(eng_[r]->ls_->grid_, 160));
     }
+    auto rate = [&](int r, int c) { return 1.0 / (kSecPerWork * work[r] / c + kSecPerEvent); };
     ncta_.assign(n, 1);
     int used = n;
-    for (int r = 0; r < n; ++r) {
-        const int lim = std::max(1, std::min(eng_[r]->ls_->grid_, 160));
-        ncta_[r] = std::max(1, std::min(lim, (int)std::floor(budget * work[r] / tot)));
-    }
-    used = 0;
-    for (int r = 0; r < n; ++r) used += ncta_[r];
-    while (used > budget) {
-        int big = 0;
-        for (int r = 1; r < n; ++r)
-            if (ncta_[r] > ncta_[big]) big = r;
-        if (ncta_[big] <= 1) break;
-        --ncta_[big];
-        --used;
+    while (used < budget) {
+        int best = -1;
+        double gain = 0.0;
+        for (int r = 0; r < n; ++r) {
+            if (ncta_[r] >= lim[r]) continue;
+            const double g = rate(r, ncta_[r] + 1) - rate(r, ncta_[r]);
+            if (g > gain) {
+                gain = g;
+                best = r;
+            }
+        }
+        if (best < 0) break;
+        ++ncta_[best];
+        ++used;
     }
     total_ctas_ = used;
     std::vector<LsArgs> plans(n);
@@ -927,6 +1076,7 @@ BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* cons
         alloc((void**)&R.mt, sizeof(rng::Mt));
         alloc((void**)&R.ctl, sizeof(BatchCtl));
         alloc((void**)&R.sel_log, sizeof(int) * kSelLog);
+        alloc((void**)&R.ev_ns, sizeof(unsigned long long) * kSelLog);
         alloc((void**)&R.ls.partials, sizeof(double) * kMaxPartials * R.ncta);
         alloc((void**)&R.ls.result, sizeof(LsResult));
         R.ls.bar = R.bar;
@@ -940,8 +1090,7 @@ BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* cons
     BCK(cudaMalloc((void**)&map_, sizeof(int2) * map.size()));
     BCK(cudaMemcpy(map_, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice));
     reps_host_ = reps;
-    first_run_.assign(n, 1);
-    remaining_.assign(n, 0.0);
+    h2d_.assign(n, 0);
 }
 
 BatchEngine::~BatchEngine() {
@@ -950,6 +1099,7 @@ BatchEngine::~BatchEngine() {
     cudaFree(alloc_reps_);
     cudaFree(map_);
     eng_.clear();
+    owned_eng_.clear();
     if (st_) cudaStreamDestroy(st_);
 }
 
@@ -987,7 +1137,7 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             std::memcpy(c.eps_macro, e.eps_macro_, sizeof(c.eps_macro));
             std::memcpy(c.sig_macro, e.sig_macro_, sizeof(c.sig_macro));
             for (int k = 0; k < 3; ++k) c.w[k] = e.ls_->w_[k];
-            c.remaining = first_run_[r] ? 0.0 : remaining_[r];
+            c.remaining = e.batch_started ? e.batch_remaining : 0.0;
             c.dt_step = std::fabs(p.step_size) / e.p_.strain_rate;
             c.strain_rate = e.p_.strain_rate;
             c.sum_two_mu = e.ls_->sum_two_mu_;
@@ -1010,14 +1160,16 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             c.n_global_steps = p.n_global_steps;
             c.elastic_done = 0;
             c.max_seq = (int)(p.max_kmc_steps_pct * (double)e.N_);
-            c.need_initial_solve = first_run_[r];
-            c.max_events = max_events > 0 ? max_events : (1LL << 62);
+            c.need_initial_solve = e.batch_started ? 0 : 1;
+            // a replica's own budget (run params) wins over the call's
+            c.max_events = p.max_events > 0 ? p.max_events : (max_events > 0 ? max_events : (1LL << 62));
             c.cascade_limit = p.max_cascade_batches > 0 ? p.max_cascade_batches : e.N_;
             c.min_margin = 1.0;
             c.sel_log_cap = kSelLog;
             c.t_start_ns = 0;
             c.limit_ns = (unsigned long long)(time_limit_s_ * 1e9);
             BCK(cudaMemcpyAsync(reps_host_[r].ctl, &c, sizeof(BatchCtl), cudaMemcpyHostToDevice, st_));
+            h2d_[r] = sizeof(BatchCtl) + sizeof(rng::Mt);
             rng::Mt mt;
             mt_from_host(e.rng_, &mt);
             BCK(cudaMemcpyAsync(reps_host_[r].mt, &mt, sizeof(rng::Mt), cudaMemcpyHostToDevice, st_));
@@ -1048,6 +1200,7 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             BCK(cudaMemcpy(&c, reps_host_[r].ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost));
             BCK(cudaMemcpy(bar, reps_host_[r].bar, sizeof(bar), cudaMemcpyDeviceToHost));
             BCK(cudaMemcpy(&mt, reps_host_[r].mt, sizeof(rng::Mt), cudaMemcpyDeviceToHost));
+            long long d2h = sizeof(BatchCtl) + sizeof(bar) + sizeof(rng::Mt);
             if (bar[2]) {
                 last_error = "device wait timed out in the batched kernel";
                 st = MGK_DEVICE_TIMEOUT;
@@ -1058,8 +1211,8 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             std::memcpy(e.sig_macro_, c.sig_macro, sizeof(c.sig_macro));
             for (int k = 0; k < 3; ++k) e.ls_->w_[k] = c.w[k], e.ls_->asym_dev2_[k] = 0.0;
             mt_to_host(mt, &e.rng_);
-            first_run_[r] = 0;
-            remaining_[r] = c.remaining;
+            e.batch_started = true;
+            e.batch_remaining = c.remaining;
             BatchStats& b = last_[r];
             b.events = c.events_done;
             b.cascades = c.cascades + (c.cascade_active ? 1 : 0);
@@ -1075,10 +1228,22 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
                 st = MGK_TIME_LIMIT;
             }
             b.ncta = ncta_[r];
+            b.sweeps = c.sweeps;
             for (int k = 0; k < 6; ++k) b.phase_ms[k] = 1e-6 * (double)c.ph_ns[k];
+            {
+                const long long ne = std::min<long long>(c.events_done, kSelLog);
+                std::vector<unsigned long long> t(ne);
+                if (ne) BCK(cudaMemcpy(t.data(), reps_host_[r].ev_ns, sizeof(unsigned long long) * ne, cudaMemcpyDeviceToHost));
+                d2h += (long long)sizeof(unsigned long long) * ne;
+                b.event_us.resize(ne);
+                for (long long i = 0; i < ne; ++i) b.event_us[i] = 1e-3 * (double)(t[i] - (i ? t[i - 1] : c.t_start_ns));
+            }
             b.sel.resize(c.sel_log_len);
             if (c.sel_log_len)
                 BCK(cudaMemcpy(b.sel.data(), reps_host_[r].sel_log, sizeof(int) * c.sel_log_len, cudaMemcpyDeviceToHost));
+            d2h += (long long)sizeof(int) * c.sel_log_len;
+            b.h2d_bytes = h2d_[r];
+            b.d2h_bytes = d2h;
             e.stats_.thermal_events += c.events_done;
             e.stats_.ls_solves += c.ls_solves;
             e.stats_.ls_iters += c.ls_iters;

@@ -17,31 +17,39 @@ struct BatchStats {
     double min_margin = 1.0;
     int terminated = 0;  // 1: instability sequence limit, 2: time limit
     int ncta = 0;
+    long long sweeps = 0;  // sweeps of every (voxel, mode) done by the run
+    long long h2d_bytes = 0, d2h_bytes = 0;  // host<->device bytes the run call copied for this replica
     double phase_ms[6] = {0, 0, 0, 0, 0, 0};  // group time in sweep, decide, event solve, cascade flips, cascade solve, interval end
     std::vector<int> sel;  // flat mode index of each thermal event, in order
+    std::vector<double> event_us;  // device time from the previous event (or the run's first decision) to each event
 };
 
 class BatchEngine {
 public:
     BatchEngine(int n, const mgk_kmc_params* params, const double* const* E, const double* const* nu);
+    // A batch over existing simulations (not owned; they must outlive the
+    // batch).  Runs advance them in place; a simulation may belong to several
+    // batches over its life, but to one running batch at a time.
+    explicit BatchEngine(const std::vector<KmcEngine*>& sims);
     ~BatchEngine();
     // Advance every replica by up to max_events thermal events (or until its
     // n_global_steps elastic steps are done); rp holds one entry per replica.
     mgk_status run(const mgk_run_params* rp, long long max_events, double* elapsed_ms);
     int size() const { return (int)eng_.size(); }
-    KmcEngine* replica(int r) { return eng_[r].get(); }
+    KmcEngine* replica(int r) { return eng_[r]; }
     const BatchStats& stats(int r) const { return last_[r]; }
     int total_ctas() const { return total_ctas_; }
     void set_time_limit(double seconds) { time_limit_s_ = seconds; }
     std::string last_error;
 
 private:
-    std::vector<std::unique_ptr<KmcEngine>> eng_;
+    void init();  // device scratch and CTA plan for eng_
+    std::vector<KmcEngine*> eng_;
+    std::vector<std::unique_ptr<KmcEngine>> owned_eng_;
     std::vector<int> ncta_;
     std::vector<void*> owned_;
     std::vector<BatchRep> reps_host_;
-    std::vector<int> first_run_;
-    std::vector<double> remaining_;
+    std::vector<long long> h2d_;
     std::vector<BatchStats> last_;
     BatchRep* alloc_reps_ = nullptr;
     int2* map_ = nullptr;

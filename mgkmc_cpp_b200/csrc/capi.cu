@@ -7,6 +7,7 @@
 
 #include "../../include/mgkmc_b200.h"
 #include "batch.cuh"
+#include "elastic.cuh"
 #include "engine.cuh"
 #include "ls.cuh"
 
@@ -210,6 +211,23 @@ mgk_status mgk_kmc_get_profile(mgk_kmc* h, double* out, double* lat, long long l
     return MGK_OK;
 }
 
+mgk_status mgk_le_run(const mgk_le_params* p, const double* E, const double* nu, double* macro_out, int* ls_iters_out) {
+    if (!p || !E || !nu) return fail(MGK_BAD_ARG, "null argument");
+    if (p->dim != 2 && p->dim != 3) return fail(MGK_BAD_ARG, "dim must be 2 or 3");
+    if (p->nx < 1 || p->ny < 1 || (p->dim == 3 && p->nz < 1)) return fail(MGK_BAD_SHAPE, "bad grid");
+    if (p->drive_i < 0 || p->drive_i >= p->dim || p->drive_j < 0 || p->drive_j >= p->dim)
+        return fail(MGK_BAD_ARG, "bad driving component");
+    if (p->n_targets < 0 || p->n_targets > 9) return fail(MGK_BAD_ARG, "n_targets out of range");
+    for (int t = 0; t < p->n_targets; ++t)
+        if (p->target_i[t] < 0 || p->target_i[t] >= p->dim || p->target_j[t] < 0 || p->target_j[t] >= p->dim)
+            return fail(MGK_BAD_ARG, "bad mixed target component");
+    if (p->max_iter_macro < 1 || p->max_iter_ls < 1) return fail(MGK_BAD_ARG, "iteration limits must be positive");
+    std::string err;
+    mgk_status s = mgk::elastic_run(*p, E, nu, macro_out, ls_iters_out, &err);
+    if (s != MGK_OK) g_err = err;
+    return s;
+}
+
 mgk_status mgk_batch_create(mgk_batch** out, int n, const mgk_kmc_params* params, const double* const* E,
                             const double* const* nu) {
     if (!out || !params || !E || !nu || n < 1) return fail(MGK_BAD_ARG, "null argument or empty batch");
@@ -227,6 +245,37 @@ mgk_status mgk_batch_create(mgk_batch** out, int n, const mgk_kmc_params* params
         return from_exception(e);
     }
     *out = h;
+    return MGK_OK;
+}
+
+mgk_status mgk_batch_create_from(mgk_batch** out, int n, mgk_kmc* const* sims) {
+    if (!out || !sims || n < 1) return fail(MGK_BAD_ARG, "null argument or empty batch");
+    *out = nullptr;
+    std::vector<mgk::KmcEngine*> v;
+    for (int r = 0; r < n; ++r) {
+        if (!sims[r] || !sims[r]->eng) return fail(MGK_BAD_ARG, "null simulation");
+        for (mgk::KmcEngine* e : v)
+            if (e == sims[r]->eng) return fail(MGK_BAD_ARG, "a simulation appears twice");
+        v.push_back(sims[r]->eng);
+    }
+    mgk_batch* h = new (std::nothrow) mgk_batch;
+    if (!h) return fail(MGK_OOM, "host allocation failed");
+    try {
+        h->b = new mgk::BatchEngine(v);
+    } catch (const std::exception& e) {
+        delete h;
+        return from_exception(e);
+    }
+    *out = h;
+    return MGK_OK;
+}
+
+mgk_status mgk_device_memory(unsigned long long* free_bytes, unsigned long long* total_bytes) {
+    size_t f = 0, t = 0;
+    cudaError_t e = cudaMemGetInfo(&f, &t);
+    if (e != cudaSuccess) return fail(MGK_CUDA_ERROR, cudaGetErrorString(e));
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
     return MGK_OK;
 }
 
@@ -249,9 +298,10 @@ mgk_status mgk_batch_run(mgk_batch* h, const mgk_run_params* rp, long long max_e
 mgk_status mgk_batch_stats(mgk_batch* h, int replica, double* out, int* sel, long long sel_cap, long long* sel_len) {
     if (!h || !out || replica < 0 || replica >= h->b->size()) return fail(MGK_BAD_ARG, "bad argument");
     const mgk::BatchStats& b = h->b->stats(replica);
-    double v[16] = {(double)b.events, (double)b.cascades, (double)b.cascade_flips, (double)b.ls_solves, (double)b.ls_iters,
+    double v[19] = {(double)b.events, (double)b.cascades, (double)b.cascade_flips, (double)b.ls_solves, (double)b.ls_iters,
                     (double)b.elastic_steps, (double)b.fallbacks, b.min_margin, (double)b.terminated, (double)b.ncta,
-                    b.phase_ms[0], b.phase_ms[1], b.phase_ms[2], b.phase_ms[3], b.phase_ms[4], b.phase_ms[5]};
+                    b.phase_ms[0], b.phase_ms[1], b.phase_ms[2], b.phase_ms[3], b.phase_ms[4], b.phase_ms[5],
+                    (double)b.sweeps, (double)b.h2d_bytes, (double)b.d2h_bytes};
     std::memcpy(out, v, sizeof(v));
     if (sel)
         for (long long i = 0; i < sel_cap && i < (long long)b.sel.size(); ++i) sel[i] = b.sel[i];
@@ -270,6 +320,15 @@ mgk_status mgk_batch_get_field(mgk_batch* h, int replica, int field, double* dst
 mgk_status mgk_batch_get_macro(mgk_batch* h, int replica, double* out, int n) {
     if (!h || !out || replica < 0 || replica >= h->b->size()) return fail(MGK_BAD_ARG, "bad argument");
     h->b->replica(replica)->get_macro(out, n);
+    return MGK_OK;
+}
+
+mgk_status mgk_batch_event_times(mgk_batch* h, int replica, double* us, long long cap, long long* len) {
+    if (!h || replica < 0 || replica >= h->b->size()) return fail(MGK_BAD_ARG, "bad argument");
+    const mgk::BatchStats& b = h->b->stats(replica);
+    if (us)
+        for (long long i = 0; i < cap && i < (long long)b.event_us.size(); ++i) us[i] = b.event_us[i];
+    if (len) *len = (long long)b.event_us.size();
     return MGK_OK;
 }
 

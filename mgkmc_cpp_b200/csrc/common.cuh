@@ -57,10 +57,20 @@ MGK_DEV dd dd_shfl_down(dd a, int o) {
 }
 
 // ---------------------------------------------------------------- grid barrier
+MGK_DEV unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// A wait at a barrier gives up after this much device time.
+constexpr unsigned long long kBarrierTimeoutNs = 30ull * 1000000000ull;
+
 // Sense-counting barrier for persistent kernels whose CTAs are co-resident
-// (launched cooperatively).  Every wait is bounded: after `limit` polls the
-// CTA records MGK_DERR_BARRIER_TIMEOUT and the barrier reports failure, so a
-// kernel never spins forever.  `bar` points at two words: {arrivals, generation}.
+// (launched cooperatively).  Every wait is bounded: after kBarrierTimeoutNs of
+// device time (or as soon as another CTA has given up) the CTA records
+// MGK_DERR_BARRIER_TIMEOUT and the barrier reports failure, so a kernel never
+// spins forever.  `bar` points at two words: {arrivals, generation}.
 struct GridBar {
     unsigned* bar;
     unsigned nblocks;
@@ -81,10 +91,12 @@ MGK_DEV bool grid_sync(const GridBar& g) {
             __threadfence();
             atomicAdd(g.bar + 1, 1u);
         } else {
-            long long polls = 0;
+            const unsigned long long t0 = global_ns();
+            unsigned polls = 0;
             while (*gen == my_gen) {
                 __nanosleep(32);
-                if ((*(volatile unsigned*)g.err & MGK_DERR_BARRIER_TIMEOUT) || ++polls > (1ll << 25)) {  // ~1-2 s
+                if ((*(volatile unsigned*)g.err & MGK_DERR_BARRIER_TIMEOUT) ||
+                    ((++polls & 255u) == 0 && global_ns() - t0 > kBarrierTimeoutNs)) {
                     atomicOr(g.err, MGK_DERR_BARRIER_TIMEOUT);
                     ok = 0;
                     break;

@@ -57,7 +57,13 @@ public:
     void set_profiling(bool on);
     const EngineProfile& profile() const { return prof_; }
     int D() const { return D_; }
+    long long N() const { return N_; }
+    long long NM() const { return NM_; }
     std::string last_error;
+    // interval state of the batched (device-resident) runs, kept with the
+    // simulation so that it may move from one batch launch to the next
+    bool batch_started = false;
+    double batch_remaining = 0.0;
 
 private:
     // enqueue an LS solve with eps_bar = eps_macro (no sync)

@@ -114,6 +114,32 @@ ENSEMBLE = ["ens2d_64"] * 16 + ["ens2d_128"] * 16 + ["ens2d_512"] * 16 + ["ens3d
     ["ens3d_96"] * 6
 
 
+SERVE_SIZES = [("2d", 32), ("2d", 64), ("2d", 128), ("2d", 256), ("2d", 512), ("3d", 32), ("3d", 64)]
+
+
+def serve_jobs(directory: str, n_jobs: int, rate: float = 20.0, seed: int = 7, flips=(500, 5000), sizes=None):
+    """The request stream of the serving case: Poisson arrivals (``rate``
+    jobs/s), each job's grid drawn uniformly from ``sizes`` (default 2D 32^2 ..
+    512^2 powers of two, 3D 32^3, 64^3), its own lognormal E field (CoV
+    uniform in [0.05, 0.2]) and seed, the reference's default barriers, and a
+    target of ``flips`` thermal events (uniform).  Returns a list of
+    (arrival_s, config, target_flips)."""
+    sizes = SERVE_SIZES if sizes is None else sizes
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for j in range(n_jobs):
+        t += rng.exponential(1.0 / rate)
+        dim, n = sizes[int(rng.integers(len(sizes)))]
+        name = "ens%s_%d" % (dim, n)
+        if name not in WORKLOADS:
+            base = WORKLOADS["ens2d_64" if dim == "2d" else "ens3d_32"]
+            WORKLOADS[name] = dict(base, nx=n, ny=n, nz=n if dim == "3d" else 1)
+        target = int(rng.integers(flips[0], flips[1] + 1))
+        out.append((t, write_workload(name, directory, seed=10000 + j)[1], target))
+    return out
+
+
 def ensemble_cov(seed: int) -> float:
     """CoV of an ensemble replica's modulus field: uniform in [0.05, 0.2]."""
     return float(np.random.default_rng(1000 + seed).uniform(0.05, 0.2))

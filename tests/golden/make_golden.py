@@ -185,5 +185,92 @@ def main():
         print("wrote", name, "rows", len(res["trace"]), "kinds", np.bincount(res["trace"][:, 0].astype(int)))
 
 
+# linear-elastic runs of the reference executable (main.cpp's
+# simulation_type "linear_elastic"): its global log (fixed 6-decimal text) and
+# the Step / Eps / Sig columns of its summary log are the fixture
+LE_CASES = {
+    "le2d_16x12_hetero": dict(dim="2d", nx=16, ny=12, nz=1, pm="plane_strain", drive="xx",
+                              targets="    yy: 0.0\n    xy: 0.0", eps_target="0.002", step="1e-4", field=True),
+    "le2d_12x10_stress_xy": dict(dim="2d", nx=12, ny=10, nz=1, pm="plane_stress", drive="xy",
+                                 targets="    xx: 0.0\n    yy: 0.05", eps_target="0.001", step="1e-4", field=True),
+    "le3d_8x6x4_hetero": dict(dim="3d", nx=8, ny=6, nz=4, pm="plane_strain", drive="zz",
+                              targets="    xx: 0.0\n    yy: 0.0", eps_target="0.0008", step="1e-4", field=True),
+}
+
+
+def le_yaml(name, epath, outdir):
+    c = LE_CASES[name]
+    return f"""seed: 1
+simulation_type: "linear_elastic"
+system:
+  dimensionality: "{c['dim']}"
+  plane_mode: "{c['pm']}"
+  nx: {c['nx']}
+  ny: {c['ny']}
+  nz: {c['nz']}
+  pixel: 1.0
+material:
+  E:
+    mode: "file"
+    parameters:
+      path: "{epath}"
+  nu:
+    mode: "constant"
+    value: 0.33
+loading:
+  eps_target: {c['eps_target']}
+  step_size: {c['step']}
+boundary_conditions:
+  driving_component: "{c['drive']}"
+  mixed_targets:
+{c['targets']}
+  mixed_tol: 1.0
+output:
+  directory: "{outdir}"
+  enable_console: false
+  enable_summary_log: true
+  enable_global_log: true
+  vtk_interval: "none"
+"""
+
+
+def le_field(name):
+    c = LE_CASES[name]
+    shape = (c["nx"], c["ny"], c["nz"]) if c["dim"] == "3d" else (c["nx"], c["ny"])
+    rng = np.random.default_rng(sum(map(ord, name)))
+    return rng.uniform(60.0, 120.0, shape)
+
+
+def summary_columns(text):
+    """Step, Eps and Sig columns of a summary log (timestamp and elapsed dropped)."""
+    rows = []
+    for line in text.splitlines()[2:]:
+        f = line.split()
+        if len(f) == 6:
+            rows.append(" ".join(f[3:]))
+    return "\n".join(rows)
+
+
+def main_le():
+    exe = os.path.abspath(os.path.join(HERE, "..", "..", "oracle", "_ref", "mgkmc_ref"))
+    for name in LE_CASES:
+        Ef = le_field(name)
+        with tempfile.TemporaryDirectory() as d:
+            np.save(os.path.join(d, "E.npy"), Ef)
+            out = os.path.join(d, "out")
+            with open(os.path.join(d, "cfg.yaml"), "w") as f:
+                f.write(le_yaml(name, os.path.join(d, "E.npy"), out))
+            subprocess.run([exe, os.path.join(d, "cfg.yaml")], check=True, capture_output=True, cwd=d, timeout=600)
+            glog = open(os.path.join(out, "global_log.txt")).read()
+            summ = summary_columns(open(os.path.join(out, "summary_log.txt")).read())
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), yaml=np.array(le_yaml(name, "$E", "$OUT")), E_gpa=Ef,
+                            global_log=np.array(glog), summary=np.array(summ))
+        print("wrote", name, glog.count("\n"), "global-log lines")
+
+
 if __name__ == "__main__":
-    main()
+    if "--le" in sys.argv:
+        main_le()
+    else:
+        main()
+        main_le()
