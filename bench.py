@@ -188,6 +188,13 @@ def sweep_bytes(cfg):
     return cfg.n_voxels * (cfg.M * 8 * (2 + C) + 8 * (2 * S + 2 + 3))
 
 
+T_START = time.time()
+
+
+def progress(msg):
+    print("[bench %7.1fs] %s" % (time.time() - T_START, msg), file=sys.stderr, flush=True)
+
+
 def percentile(x, q):
     return float(np.percentile(x, q)) if len(x) else None
 
@@ -202,9 +209,12 @@ def ensemble_block(G, workloads, workdir, seconds, plain_events):
     cfgs = [c for _, _, c in reps]
     b = G.KmcBatch(cfgs)
     t_setup = time.time() - t0
-    b.run(3)
+    progress("ensemble: %d replicas set up in %.1f s" % (len(cfgs), t_setup))
     b.set_time_limit(seconds)
+    b.run(3)
+    progress("ensemble: warm-up done")
     ms = b.run(10 ** 9)
+    progress("ensemble: timed run %.1f s" % (ms / 1e3))
     st = [b.stats(r) for r in range(len(cfgs))]
     events = sum(x["events"] for x in st)
     vox_iters = sum(x["ls_iters"] * c.n_voxels for x, c in zip(st, cfgs))
@@ -229,6 +239,7 @@ def ensemble_block(G, workloads, workdir, seconds, plain_events):
         ev = sim.stats["thermal_events"] - e0
         rate = ev / (sim.profile()["run_ms"] / 1e3) if ev else 0.0
         k["plain_steps_per_s"] = rate
+        progress("ensemble: plain %s %.1f steps/s" % (name, rate))
         if rate > 0:
             plain_time += k["events"] / rate
         del sim
@@ -261,14 +272,18 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_events=50):
             time.sleep(min(0.05, srv.queue[0]["arrival"] - now))
             continue
         dev_ms += srv.step(now)
+        if srv.launches % 20 == 0:
+            progress("serving: %d launches, %d active, %d queued, %d done" % (srv.launches, len(srv.active),
+                                                                                len(srv.queue), len(srv.done)))
     wall = time.perf_counter() - t0
     done = list(srv.done.values())
     events = sum(j["events"] for j in done)
+    stalled = sum(1 for j in done if j["stalled"])
     comp = [j["finished"] - j["arrival"] for j in done]
     lat = np.array(srv.step_latency_us)
     return {"jobs": len(done), "arrivals": "Poisson 20 jobs/s, seed 7", "flips_per_job": list(flips),
             "sizes": ["%s %d" % x for x in sizes], "slice_events": slice_events, "events": int(events),
-            "wall_seconds": wall, "device_seconds": dev_ms / 1e3, "launches": srv.launches,
+            "wall_seconds": wall, "device_seconds": dev_ms / 1e3, "launches": srv.launches, "stalled_jobs": stalled,
             "value": events / wall if wall > 0 else None, "unit": UNIT,
             "step_latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},
             "job_completion_s": {"p50": percentile(comp, 50), "p99": percentile(comp, 99)}}
@@ -356,6 +371,7 @@ def main():
             dist.barrier()
 
     # chosen form: all replicas in one device-resident launch
+    progress("chosen form: %d replicas" % len(cfgs))
     batch = G.KmcBatch(cfgs)
     batch.run(args.warmup)
     clocks = ClockSampler(local_rank)
@@ -389,6 +405,7 @@ def main():
     batch.close()
 
     # plain form: the drop-in engine, one replica (seed of this rank's first replica)
+    progress("plain form")
     sim = G.from_config(cfg, output_dir=os.path.join(workdir, "out"))
     kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
 
@@ -418,12 +435,14 @@ def main():
     del sim
 
     ens = None
+    progress("ensemble")
     if not args.no_ensemble and rank == 0:
         try:
             ens = ensemble_block(G, workloads, workdir, args.ensemble_seconds, 20)
         except Exception as e:  # reported, never silently dropped
             ens = {"error": str(e)[-300:]}
     srv = None
+    progress("serving")
     if args.serve_jobs > 0 and rank == 0:
         sizes = workloads.SERVE_SIZES if args.serve_full_sizes else [x for x in workloads.SERVE_SIZES
                                                                      if x in (("2d", 32), ("2d", 64), ("2d", 128),
@@ -478,6 +497,7 @@ def main():
     if srv is not None:
         line["serving"] = srv
     if args.gpus == 1:
+        progress("cpu baseline")
         res, err = run_reference(cfg_paths, args.cpu_events)
         if res is not None:
             line["cpu_baseline"] = {"value": res["value"], "unit": UNIT, "cores": len(cfg_paths), "kind": "reference",

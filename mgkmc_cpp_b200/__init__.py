@@ -416,16 +416,18 @@ class Server:
     memory when the server starts, less ``reserve_bytes``), and the device
     has that much free right now.  Admitted jobs keep their fields and random
     stream resident on the device.  The step then advances every active job
-    by up to ``slice_events`` events in one batched launch and retires the
-    jobs that reached their target.  A job's trajectory does not depend on
+    by up to ``slice_events`` events in one batched launch (each launch
+    bounded by ``time_limit`` seconds) and retires the jobs that reached their
+    target (or made no progress in ``max_stalls`` slices in a row).  A job's trajectory does not depend on
     what shares its launches: its random stream and interval clock are its
     own."""
 
-    def __init__(self, max_active=64, slice_events=50, reserve_bytes=8 << 30, hbm_budget=None, time_limit=60.0):
+    def __init__(self, max_active=64, slice_events=50, reserve_bytes=8 << 30, hbm_budget=None, time_limit=10.0,
+                 max_stalls=3):
         self.max_active, self.slice_events, self.reserve = int(max_active), int(slice_events), int(reserve_bytes)
         self.budget = int(hbm_budget) if hbm_budget is not None else device_memory()[0] - self.reserve
         self.committed = 0
-        self.time_limit = float(time_limit)
+        self.time_limit, self.max_stalls = float(time_limit), int(max_stalls)
         self.queue, self.active, self.done = [], [], {}
         self._next = 0
         self.launches = 0
@@ -435,7 +437,8 @@ class Server:
         jid = self._next
         self._next += 1
         self.queue.append({"id": jid, "cfg": cfg, "target": int(flips), "events": 0, "selected": [],
-                           "arrival": float(arrival), "admitted": None, "finished": None, "latency_us": []})
+                           "arrival": float(arrival), "admitted": None, "finished": None, "latency_us": [],
+                           "stalls": 0, "stalled": False})
         return jid
 
     def _admit(self, now: float):
@@ -469,7 +472,11 @@ class Server:
             job["selected"].append(st["selected"])
             job["latency_us"].extend(st["event_us"].tolist())
             self.step_latency_us.extend(st["event_us"].tolist())
-            if job["events"] >= job["target"] or st["terminated"]:
+            # a job whose slices end without an event (a cascade that does not
+            # settle within the slice's time limit) is retired after max_stalls
+            job["stalls"] = job["stalls"] + 1 if st["events"] == 0 else 0
+            job["stalled"] = job["stalls"] >= self.max_stalls
+            if job["events"] >= job["target"] or st["terminated"] or job["stalled"]:
                 job["finished"] = now
                 job["selected"] = np.concatenate(job["selected"]) if job["selected"] else np.zeros(0, np.int64)
                 job["eps_field"] = job["sim"].eps_field

@@ -56,3 +56,40 @@ def compare_trace(tr, ref, tol=1e-9):
     err = np.abs(tr[:, 3:] - ref[:, 3:]) / scale
     assert err.max() <= tol, (err.max(), np.unravel_index(np.argmax(err), err.shape))
     assert np.allclose(tr[~ev, 1], ref[~ev, 1], rtol=0, atol=0)
+
+
+def _close_token(a, b):
+    """Two printed numbers agree to one unit of the last printed digit
+    (fixed notation) or 2e-6 relative (exponent notation); other tokens must
+    be equal."""
+    if a == b:
+        return True
+    try:
+        x, y = float(a), float(b)
+    except ValueError:
+        return False
+    if "e" in b.lower():
+        return abs(x - y) <= 2e-6 * max(abs(y), 1e-300)
+    dec = len(b.split(".")[1]) if "." in b else 0
+    return abs(x - y) <= 1.01 * 10.0 ** (-dec)
+
+
+def same_log(ours, ref, skip_prefix=2):
+    """Logs with the same lines and columns; numbers within one unit of their
+    last printed digit (components that are zero up to rounding noise may
+    print as -0.000 on one side).  The first skip_prefix tokens of lines that
+    start with a date (timestamp and elapsed seconds) and the run-time
+    trailer lines are not compared."""
+    import re
+    a = [l for l in ours.splitlines() if not l.startswith(("Simulation Finish", "Total Duration"))]
+    b = [l for l in ref.splitlines() if not l.startswith(("Simulation Finish", "Total Duration"))]
+    assert len(a) == len(b), (len(a), len(b))
+    for la, lb in zip(a, b):
+        if la == lb:
+            continue
+        fa, fb = la.split(), lb.split()
+        if re.match(r"\d{4}-\d\d-\d\d", lb):
+            fa, fb = fa[skip_prefix + 1:], fb[skip_prefix + 1:]
+        assert len(fa) == len(fb), (la, lb)
+        for x, y in zip(fa, fb):
+            assert _close_token(x, y), (x, y, la, lb)

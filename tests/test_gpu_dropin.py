@@ -1,0 +1,104 @@
+"""Drop-in check: the reference's own main.cpp, unmodified, compiled against
+this project's replacement headers (include/shim/kmc_solver.hpp,
+include/shim/linear_elastic_solver.hpp) and libmgkmc_b200
+(oracle/_ref/mgkmc_dropin, built by oracle/Makefile), must write the same logs
+as the reference executable (oracle/_ref/mgkmc_ref) on the same config file:
+a KMC run with thermal events, a cascade and elastic steps, and the
+linear-elastic runs of the golden fixtures."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import golden, same_log
+
+pytestmark = pytest.mark.gpu
+
+REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+
+KMC_YAML = """seed: 5
+simulation_type: "kmc"
+system:
+  dimensionality: "2d"
+  plane_mode: "plane_strain"
+  nx: 16
+  ny: 16
+  pixel: 1.0
+  M: 6
+  gamma0: 0.1
+material:
+  E:
+    mode: "constant"
+    value: 90
+  nu:
+    mode: "constant"
+    value: 0.36
+loading:
+  eps_target: 2e-5
+  step_size: 1e-6
+boundary_conditions:
+  driving_component: "xx"
+  mixed_targets:
+    yy: 0.0
+    xy: 0.0
+  mixed_tol: 1.0
+barriers:
+  type: "gaussian"
+  kwargs:
+    mean: 2.0
+    std: 0.6
+    min_cutoff: 0.1
+physics:
+  enable_softening: true
+  softening_scheme: "isotropic"
+  jp: 1.0
+  jt: 3.0
+  softening_cap: 0.5
+dynamics:
+  instability_mode: "cascade"
+  temperature: 300
+  nu0: 1e13
+  physical_strain_rate: 0.1
+output:
+  directory: "$OUT"
+  enable_console: false
+  vtk_interval: "none"
+"""
+
+
+def run(exe, text, d):
+    cfg = os.path.join(d, "cfg.yaml")
+    with open(cfg, "w") as f:
+        f.write(text)
+    r = subprocess.run([os.path.join(REF, exe), cfg], cwd=d, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:] + r.stdout[-2000:]
+
+
+def binaries():
+    for exe in ("mgkmc_ref", "mgkmc_dropin"):
+        if not os.path.exists(os.path.join(REF, exe)):
+            pytest.skip("oracle/_ref/%s not built (needs the reference sources at build time)" % exe)
+
+
+def test_dropin_kmc_logs_match_reference(tmp_path):
+    binaries()
+    outs = {}
+    for exe in ("mgkmc_ref", "mgkmc_dropin"):
+        d = tmp_path / exe
+        d.mkdir()
+        run(exe, KMC_YAML.replace("$OUT", str(d / "out")), str(d))
+        outs[exe] = {f: open(d / "out" / f).read() for f in ("summary_log.txt", "global_log.txt")}
+    for f in ("summary_log.txt", "global_log.txt"):
+        same_log(outs["mgkmc_dropin"][f], outs["mgkmc_ref"][f])
+    assert "CASCADE" in outs["mgkmc_ref"]["summary_log.txt"] and "KMC" in outs["mgkmc_ref"]["summary_log.txt"]
+
+
+@pytest.mark.parametrize("name", ["le2d_16x12_hetero", "le3d_8x6x4_hetero"])
+def test_dropin_linear_elastic_logs_match_reference(name, tmp_path):
+    binaries()
+    g = golden(name)
+    np.save(tmp_path / "E.npy", g["E_gpa"])
+    run("mgkmc_dropin", str(g["yaml"]).replace("$E", str(tmp_path / "E.npy")).replace("$OUT", str(tmp_path / "out")),
+        str(tmp_path))
+    same_log(open(tmp_path / "out" / "global_log.txt").read(), str(g["global_log"]))
