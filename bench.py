@@ -254,14 +254,14 @@ def ensemble_block(G, workloads, workdir, seconds, plain_events):
             "per_class": classes, "setup_seconds": t_setup}
 
 
-def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_events=50):
+def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05):
     """The serving loop on a Poisson request stream (20 jobs/s, seed 7): jobs
     are admitted as they arrive (wall clock) and as memory allows, every
-    active job advances in shared batched launches of slice_events events,
-    finished jobs retire.  Returns throughput, per-step latency and job
+    active job advances in shared batched launches of slice_seconds of device
+    time, finished jobs retire.  Returns throughput, per-step latency and job
     completion latency."""
     jobs = workloads.serve_jobs(os.path.join(workdir, "serve"), n_jobs, flips=flips, sizes=sizes)
-    srv = G.Server(slice_events=slice_events)
+    srv = G.Server(slice_seconds=slice_seconds)
     for arrival, cfg, target in jobs:
         srv.submit(cfg, target, arrival=arrival)
     t0 = time.perf_counter()
@@ -282,7 +282,7 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_events=50):
     comp = [j["finished"] - j["arrival"] for j in done]
     lat = np.array(srv.step_latency_us)
     return {"jobs": len(done), "arrivals": "Poisson 20 jobs/s, seed 7", "flips_per_job": list(flips),
-            "sizes": ["%s %d" % x for x in sizes], "slice_events": slice_events, "events": int(events),
+            "sizes": ["%s %d" % x for x in sizes], "slice_seconds": slice_seconds, "events": int(events),
             "wall_seconds": wall, "device_seconds": dev_ms / 1e3, "launches": srv.launches, "stalled_jobs": stalled,
             "value": events / wall if wall > 0 else None, "unit": UNIT,
             "step_latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},

@@ -32,7 +32,7 @@ typedef enum {
     MGK_DEVICE_TIMEOUT = 4,   /* a bounded device wait gave up */
     MGK_CUDA_ERROR = 5,
     MGK_BAD_ARG = 6,
-    MGK_UNSUPPORTED = 7,      /* option not built (e.g. fast patching) */
+    MGK_UNSUPPORTED = 7,      /* option not built (e.g. fast patching in the batched form) */
     MGK_TERMINATED = 8,       /* KMC instability sequence limit (kmc_solver.hpp:925-929) */
     MGK_TIME_LIMIT = 9        /* a batched run reached its wall-time limit (mgk_batch_set_time_limit) */
 } mgk_status;
@@ -112,7 +112,8 @@ typedef struct {
     double temperature, strain_rate, stability_threshold, nu0;
     int instability_kmc;      /* instability_mode == "kmc" (else "cascade") */
     int scale_rate_by_volume, redraw_directions, redraw_barriers, use_3d_barriers;
-    int fast_patching, patch_radius, sync_interval; /* fast patching: MGK_UNSUPPORTED */
+    int fast_patching, patch_radius, sync_interval; /* kmc_solver.hpp:276-332, 866-913: stencil stress updates,
+                                                        a full LS solve every sync_interval flips (plain form only) */
     double ls_tol;            /* elastic_run tolerance, reference 1e-6 (:337) */
     int ls_max_iter;          /* reference 200 */
 } mgk_kmc_params;

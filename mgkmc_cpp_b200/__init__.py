@@ -416,18 +416,21 @@ class Server:
     memory when the server starts, less ``reserve_bytes``), and the device
     has that much free right now.  Admitted jobs keep their fields and random
     stream resident on the device.  The step then advances every active job
-    by up to ``slice_events`` events in one batched launch (each launch
-    bounded by ``time_limit`` seconds) and retires the jobs that reached their
-    target (or made no progress in ``max_stalls`` slices in a row).  A job's trajectory does not depend on
+    in one batched launch for ``slice_seconds`` of device time (or by
+    ``slice_events`` events each, when given) and retires the jobs that
+    reached their target (or made no progress for ``stall_seconds``).  A job's trajectory does not depend on
     what shares its launches: its random stream and interval clock are its
     own."""
 
-    def __init__(self, max_active=64, slice_events=50, reserve_bytes=8 << 30, hbm_budget=None, time_limit=10.0,
-                 max_stalls=3):
-        self.max_active, self.slice_events, self.reserve = int(max_active), int(slice_events), int(reserve_bytes)
+    def __init__(self, max_active=64, slice_events=None, slice_seconds=0.05, reserve_bytes=8 << 30, hbm_budget=None,
+                 stall_seconds=30.0):
+        self.max_active, self.reserve = int(max_active), int(reserve_bytes)
+        self.slice_events = None if slice_events is None else int(slice_events)
+        self.slice_seconds = float(slice_seconds)
         self.budget = int(hbm_budget) if hbm_budget is not None else device_memory()[0] - self.reserve
         self.committed = 0
-        self.time_limit, self.max_stalls = float(time_limit), int(max_stalls)
+        self.stall_seconds = float(stall_seconds)
+        self._batch, self._batch_ids = None, None
         self.queue, self.active, self.done = [], [], {}
         self._next = 0
         self.launches = 0
@@ -438,7 +441,7 @@ class Server:
         self._next += 1
         self.queue.append({"id": jid, "cfg": cfg, "target": int(flips), "events": 0, "selected": [],
                            "arrival": float(arrival), "admitted": None, "finished": None, "latency_us": [],
-                           "stalls": 0, "stalled": False})
+                           "idle_s": 0.0, "stalled": False})
         return jid
 
     def _admit(self, now: float):
@@ -459,11 +462,24 @@ class Server:
         self._admit(now)
         if not self.active:
             return 0.0
-        b = KmcBatch(sims=[j["sim"] for j in self.active])
-        b.cfgs = [j["cfg"] for j in self.active]
-        b.set_time_limit(self.time_limit)
-        ms = b.run(self.slice_events,
-                   budgets=[min(self.slice_events, j["target"] - j["events"]) for j in self.active])
+        ids = [j["id"] for j in self.active]
+        if ids != self._batch_ids:  # the active set changed: a new batch (CTA plan) over the resident jobs
+            if self._batch is not None:
+                self._batch.close()
+            self._batch = KmcBatch(sims=[j["sim"] for j in self.active])
+            self._batch.cfgs = [j["cfg"] for j in self.active]
+            self._batch_ids = ids
+        b = self._batch
+        # a slice is a device-time budget (every job stops at its first
+        # decision past it, so a large job never holds the small ones back),
+        # or a fixed number of events per job when slice_events is set
+        if self.slice_events is None:
+            b.set_time_limit(self.slice_seconds)
+            budgets = [j["target"] - j["events"] for j in self.active]
+        else:
+            b.set_time_limit(60.0)
+            budgets = [min(self.slice_events, j["target"] - j["events"]) for j in self.active]
+        ms = b.run(max(budgets), budgets=budgets)
         self.launches += 1
         keep = []
         for r, job in enumerate(self.active):
@@ -472,11 +488,11 @@ class Server:
             job["selected"].append(st["selected"])
             job["latency_us"].extend(st["event_us"].tolist())
             self.step_latency_us.extend(st["event_us"].tolist())
-            # a job whose slices end without an event (a cascade that does not
-            # settle within the slice's time limit) is retired after max_stalls
-            job["stalls"] = job["stalls"] + 1 if st["events"] == 0 else 0
-            job["stalled"] = job["stalls"] >= self.max_stalls
-            if job["events"] >= job["target"] or st["terminated"] or job["stalled"]:
+            # a job without an event for stall_seconds of device time (a
+            # cascade that does not settle) is retired as stalled
+            job["idle_s"] = job["idle_s"] + ms / 1e3 if st["events"] == 0 else 0.0
+            job["stalled"] = job["idle_s"] >= self.stall_seconds
+            if job["events"] >= job["target"] or st["terminated"] == 1 or job["stalled"]:
                 job["finished"] = now
                 job["selected"] = np.concatenate(job["selected"]) if job["selected"] else np.zeros(0, np.int64)
                 job["eps_field"] = job["sim"].eps_field
@@ -487,7 +503,9 @@ class Server:
                 self.done[job["id"]] = job
             else:
                 keep.append(job)
-        b.close()
+        if len(keep) != len(self.active):
+            b.close()
+            self._batch, self._batch_ids = None, None
         self.active = keep
         return ms
 

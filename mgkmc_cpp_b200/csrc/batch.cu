@@ -984,6 +984,8 @@ BatchEngine::BatchEngine(const std::vector<KmcEngine*>& sims) : eng_(sims) {
 
 void BatchEngine::init() {
     const int n = (int)eng_.size();
+    for (KmcEngine* e : eng_)
+        if (e->fp_) throw std::domain_error("fast patching runs in the plain form (mgk_kmc_run) only");
     BCK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);

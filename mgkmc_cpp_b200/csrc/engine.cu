@@ -94,7 +94,8 @@ static bool dbg() {
 KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu) : p_(p), rng_((unsigned)p.seed) {
     if (p.dim != 2 && p.dim != 3) throw std::invalid_argument("dim must be 2 or 3");
     if (p.nx < 1 || p.ny < 1 || (p.dim == 3 && p.nz < 1) || p.M < 1) throw std::invalid_argument("bad grid or M");
-    if (p.fast_patching) throw std::domain_error("fast patching is not built in this library");
+    if (p.fast_patching && (p.patch_radius < 0 || p.sync_interval < 1))
+        throw std::invalid_argument("fast patching needs patch_radius >= 0 and sync_interval >= 1");
     D_ = p.dim;
     S_ = D_ == 2 ? 3 : 6;
     C_ = (D_ == 3 && p.use_3d_barriers) ? 6 : 2;
@@ -186,6 +187,114 @@ KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu)
     alloc((void**)&d_cmodes_, sizeof(int) * N);
     alloc((void**)&d_ckeys2_, sizeof(double) * npow2);
     alloc((void**)&d_cmodes2_, sizeof(int) * npow2);
+    if (p.fast_patching) {
+        fp_ = true;
+        fp_R_ = p.patch_radius;
+        fp_sync_ = p.sync_interval;
+        alloc((void**)&dev_.sig_s, sizeof(double) * S_ * N);
+        alloc((void**)&dev_.flipcat, sizeof(double) * C_ * N);
+        alloc((void**)&d_unit_, sizeof(double) * S_);
+        CK(cudaMemset(dev_.sig_s, 0, sizeof(double) * S_ * N));
+        aux_.reset(new LsSolver(D_, dims, p.plane_stress != 0, p.pixel, E, nu, st_));
+        precompute_patches();
+    }
+}
+
+// precompute_patch_kernels (kmc_solver.hpp:276-332 / :1256-1331): the stress
+// of a unit deviatoric eigenstrain at the centre voxel, for every basis,
+// cropped to (2R+1)^D around it, plus the mean the crop misses.
+void KmcEngine::precompute_patches() {
+    const int D = D_, S = S_, R = fp_R_;
+    const int nx = p_.nx, ny = p_.ny, nz = D == 3 ? p_.nz : 1;
+    const int nb = D == 2 ? 2 : 5, side = 2 * R + 1, side_z = (D == 3 && nz > 1) ? side : 1;
+    const long P = (long)side * side * side_z;
+    const long N = N_;
+    const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+    const long centre = ((long)cx * ny + cy) * nz + cz;
+    // bases in symmetric components (2D: xx, yy, xy; 3D: xx, yy, zz, xy, xz, yz)
+    static const double b2[2][3] = {{1, -1, 0}, {0, 0, 1}};
+    static const double b3[5][6] = {{1, -1, 0, 0, 0, 0}, {0, 1, -1, 0, 0, 0}, {0, 0, 0, 1, 0, 0}, {0, 0, 0, 0, 1, 0},
+                                    {0, 0, 0, 0, 0, 1}};
+    static const int sym2[4] = {0, 2, 2, 1};
+    static const int sym3[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+    std::vector<double> K((size_t)nb * P * S), miss((size_t)nb * S), sig((size_t)N * D * D);
+    double* d_ep = nullptr;
+    CK(cudaMalloc((void**)&d_ep, sizeof(double) * S * N));
+    const double zero[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < nb; ++b) {
+        CK(cudaMemsetAsync(d_ep, 0, sizeof(double) * S * N, st_));
+        for (int c = 0; c < S; ++c) {
+            const double v = D == 2 ? b2[b][c] : b3[b][c];
+            CK(cudaMemcpyAsync(d_ep + (long)c * N + centre, &v, sizeof(double), cudaMemcpyHostToDevice, st_));
+            CK(cudaStreamSynchronize(st_));
+        }
+        CK(aux_->solve(zero, false, d_ep, 200, 1e-6));
+        CK(cudaStreamSynchronize(st_));
+        if (aux_->device_error()) throw std::runtime_error("device wait timed out in the LS solver");
+        CK(aux_->download_sig(d_ep, sig.data()));
+        double sum_crop[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int dx = -R; dx <= R; ++dx)
+            for (int dy = -R; dy <= R; ++dy)
+                for (int dz = (side_z > 1 ? -R : 0); dz <= (side_z > 1 ? R : 0); ++dz) {
+                    const long sx = ((cx + dx) % nx + nx) % nx, sy = ((cy + dy) % ny + ny) % ny,
+                               sz = ((cz + dz) % nz + nz) % nz;
+                    const double* val = &sig[(size_t)((sx * ny + sy) * nz + sz) * D * D];
+                    const long crop = ((long)(dx + R) * side + (dy + R)) * side_z + (side_z > 1 ? dz + R : 0);
+                    for (int k = 0; k < D * D; ++k) {
+                        const int c = D == 2 ? sym2[k] : sym3[k];
+                        if (k / D <= k % D) K[((size_t)b * P + crop) * S + c] = val[k];
+                        sum_crop[k] += val[k];
+                    }
+                }
+        double sum_sig[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (long i = 0; i < N; ++i)
+            for (int k = 0; k < D * D; ++k) sum_sig[k] += sig[(size_t)i * D * D + k];
+        for (int k = 0; k < D * D; ++k) {
+            if (k / D > k % D) continue;
+            const double mean = sum_sig[k] / (double)N;
+            miss[(size_t)b * S + (D == 2 ? sym2[k] : sym3[k])] = mean - sum_crop[k] / (double)N;
+        }
+    }
+    cudaFree(d_ep);
+    CK(cudaMalloc((void**)&d_patchK_, sizeof(double) * K.size()));
+    CK(cudaMalloc((void**)&d_patchMiss_, sizeof(double) * miss.size()));
+    CK(cudaMemcpy(d_patchK_, K.data(), sizeof(double) * K.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_patchMiss_, miss.data(), sizeof(double) * miss.size(), cudaMemcpyHostToDevice));
+}
+
+// After the flips of d_modes[0..nflips) (their pre-redraw catalog entries in
+// dev_.flipcat): on the first thermal flip the macroscopic stress of a unit
+// driving strain (sigma_macro_unit, one side solve); then the predictor
+// (pred = strain_rate * t_wait, 0 for none) and the stencils.  Cascade flips
+// (thermal false) add stencils only.
+mgk_status KmcEngine::patch_after_flips(const int* d_modes, int nflips, double pred, bool thermal, int comp_i,
+                                        int comp_j) {
+    if (thermal && !unit_init_) {
+        double eb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, em[9], sm[9];
+        eb[comp_i * D_ + comp_j] = 1.0;
+        CK(aux_->solve(eb, false, nullptr, 200, 1e-6));
+        LsResult r;
+        CK(cudaMemcpyAsync(&r, aux_->device_result(), sizeof(LsResult), cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+        if (aux_->device_error()) {
+            last_error = "device wait timed out in the LS solver";
+            return MGK_DEVICE_TIMEOUT;
+        }
+        const_cast<LsResult&>(aux_->host_result()) = r;
+        int it = 0;
+        aux_->macro(em, sm, &it);
+        double u[6];
+        if (D_ == 2) {
+            u[0] = sm[0], u[1] = sm[3], u[2] = sm[1];
+        } else {
+            u[0] = sm[0], u[1] = sm[4], u[2] = sm[8], u[3] = sm[1], u[4] = sm[2], u[5] = sm[5];
+        }
+        CK(cudaMemcpy(d_unit_, u, sizeof(double) * S_, cudaMemcpyHostToDevice));
+        unit_init_ = true;
+    }
+    stats_.launches += 1;
+    CK(kmc_patch(dev_, phys_, d_modes, nflips, d_patchK_, d_patchMiss_, fp_R_, d_unit_, unit_init_ ? pred : 0.0, st_));
+    return MGK_OK;
 }
 
 KmcEngine::~KmcEngine() {
@@ -208,6 +317,11 @@ KmcEngine::~KmcEngine() {
     cudaFree(d_cmodes_);
     cudaFree(d_ckeys2_);
     cudaFree(d_cmodes2_);
+    cudaFree(dev_.sig_s);
+    cudaFree(dev_.flipcat);
+    cudaFree(d_unit_);
+    cudaFree(d_patchK_);
+    cudaFree(d_patchMiss_);
     cudaFreeHost(h_status_);
     cudaFreeHost(h_upload_);
     cudaFreeHost(h_lsres_);
@@ -327,6 +441,10 @@ cudaError_t KmcEngine::enqueue_elastic() {
     stats_.launches += 1;
     cudaError_t e = ls_->solve(eps_macro_, true, dev_.epsp_s, p_.ls_max_iter, p_.ls_tol);
     prof_end(0);
+    if (e == cudaSuccess && fp_) {
+        stats_.launches += 1;
+        e = kmc_stress(dev_, st_);  // the kept stress restarts from the solve
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_lsres_, ls_->device_result(), sizeof(LsResult), cudaMemcpyDeviceToHost, st_);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_lserr_, ls_->device_error_ptr(), sizeof(unsigned), cudaMemcpyDeviceToHost, st_);
     ls_pending_ = true;
@@ -432,7 +550,14 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips, long long cap) {
             while ((1 << lg) < np2) ++lg;
             stats_.launches += 1 + (np2 <= 8192 ? 1 : 1 + lg * (lg + 1) / 2);
         }
-        CK(enqueue_elastic());
+        if (fp_) {  // stencils per flip, in flip order; the LS solve after the cascade (kmc_solver.hpp:525-560)
+            int np2 = 1;
+            while (np2 < n) np2 <<= 1;
+            mgk_status ps = patch_after_flips(np2 <= 8192 ? d_cmodes_ : d_cmodes2_, n, 0.0, false, 0, 0);
+            if (ps != MGK_OK) return ps;
+        } else {
+            CK(enqueue_elastic());
+        }
         if (dbg()) fprintf(stderr, "[mgk] cascade batch %d flips %d\n", local, n);
         total += n;
         ++local;
@@ -440,6 +565,12 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips, long long cap) {
         mgk_status s = sync_status();
         if (s != MGK_OK) return s;
         if (local > limit) break;
+    }
+    if (fp_ && total > 0) {
+        CK(enqueue_elastic());
+        CK(enqueue_sweep());
+        mgk_status s = sync_status();
+        if (s != MGK_OK) return s;
     }
     *steps = local;
     *flips = total;
@@ -644,7 +775,20 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                         CK(kmc_select_flip(dev_, phys_, d_blk_, d_blk_last_, nblk_, items_, d_upload_, time_, d_upload_ + 1,
                                            p_.redraw_directions, p_.redraw_barriers, d_status_, st_));
                         prof_end(2);
-                        CK(enqueue_elastic());
+                        if (fp_) {  // kmc_solver.hpp:866-915: predictor, stencil, LS only every sync_interval flips
+                            s = patch_after_flips(&d_status_->selected, 1, tw > 0.0 ? p_.strain_rate * tw : 0.0, true,
+                                                  rp.comp_i, rp.comp_j);
+                            if (s != MGK_OK) {
+                                close_logs();
+                                return s;
+                            }
+                            if (++flips_since_sync_ >= fp_sync_) {
+                                CK(enqueue_elastic());
+                                flips_since_sync_ = 0;
+                            }
+                        } else {
+                            CK(enqueue_elastic());
+                        }
                         CK(enqueue_sweep());
                         s = sync_status();
                         if (s != MGK_OK) {
@@ -806,6 +950,22 @@ mgk_status KmcEngine::get_field(int field, double* dst, long long* count) {
     try {
         if (field == 0) {
             CK(ls_->download_eps(dst));
+        } else if (field == 1 && fp_) {
+            // the kept (patched) stress field: its symmetric part, plus the
+            // antisymmetric part of the last LS solve's stress (2 mu w, from
+            // an applied strain with unequal off-diagonal halves)
+            CK(ls_->download_sig(dev_.epsp_s, dst));
+            std::vector<double> s((size_t)S_ * N);
+            CK(cudaMemcpy(s.data(), dev_.sig_s, sizeof(double) * S_ * N, cudaMemcpyDeviceToHost));
+            static const int m2[4] = {0, 2, 2, 1};
+            static const int m3[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+            for (long v = 0; v < N; ++v) {
+                double* o = dst + v * DD;
+                double a[9];
+                for (int i = 0; i < D; ++i)
+                    for (int j = 0; j < D; ++j) a[i * D + j] = 0.5 * (o[i * D + j] - o[j * D + i]);
+                for (int k = 0; k < DD; ++k) o[k] = s[(size_t)(D == 2 ? m2[k] : m3[k]) * N + v] + a[k];
+            }
         } else if (field == 1) {
             CK(ls_->download_sig(dev_.epsp_s, dst));
         } else if (field == 2) {

@@ -78,6 +78,9 @@ private:
     void log_line(int global_step, int elastic_steps_done, int total_kmc, const char* type, int csteps, int cflips);
     void maybe_vtk(int global_step, int elastic_steps_done, const char* type, bool init);
     void export_vtu(const std::string& name);
+    // fast patching (kmc_solver.hpp:276-332 / :1256-1331, 866-913 / :1877-1939)
+    void precompute_patches();
+    mgk_status patch_after_flips(const int* d_modes, int nflips, double pred, bool thermal, int comp_i, int comp_j);
 
     mgk_kmc_params p_;
     int D_, S_, C_, M_, N_;
@@ -103,6 +106,11 @@ private:
     double *d_ckeys_ = nullptr, *d_ckeys2_ = nullptr;
     int *d_cmodes_ = nullptr, *d_cmodes2_ = nullptr;
     LsResult* h_lsres_ = nullptr;    // pinned copy of the last LS result
+    bool fp_ = false;                 // fast patching
+    int fp_R_ = 5, fp_sync_ = 100, flips_since_sync_ = 0;
+    bool unit_init_ = false;          // sigma_macro_unit computed
+    std::unique_ptr<LsSolver> aux_;   // the reference's side solves (patch kernels, unit macro stress)
+    double *d_patchK_ = nullptr, *d_patchMiss_ = nullptr, *d_unit_ = nullptr;
     bool ls_pending_ = false;
     EngineStats stats_;
     // profiling

@@ -29,9 +29,10 @@ MGK_DEV void cat_sym(const double* c, double* o) {
     }
 }
 
-// Q of mode i at voxel v (update_barriers, kmc_solver.hpp:345-407 / :1344-1406)
-template <int D, int C>
-MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, double time) {
+// Stress of voxel v from the LS strain (stress_from_strain_2d/3d,
+// linear_elastic_solver.hpp:48-67 / :322-341), symmetric components.
+template <int D>
+MGK_DEV void voxel_stress(const KmcDevState& s, int v, double* sg) {
     constexpr int S = D == 2 ? 3 : 6;
     const int N = s.N;
     double e[S];
@@ -41,9 +42,22 @@ MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, dou
 #pragma unroll
     for (int c = 0; c < D; ++c) tr += e[c];
     const double m2 = 2.0 * s.mu[v], l = s.lam[v];
-    double sg[S];
 #pragma unroll
     for (int c = 0; c < S; ++c) sg[c] = m2 * e[c] + (c < D ? l * tr : 0.0);
+}
+
+// Q of mode i at voxel v (update_barriers, kmc_solver.hpp:345-407 / :1344-1406)
+template <int D, int C>
+MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, double time) {
+    constexpr int S = D == 2 ? 3 : 6;
+    const int N = s.N;
+    double sg[S];
+    if (s.sig_s) {  // fast patching: the kept stress field
+#pragma unroll
+        for (int c = 0; c < S; ++c) sg[c] = s.sig_s[(long)c * N + v];
+    } else {
+        voxel_stress<D>(s, v, sg);
+    }
     // softening state
     const double gt = s.soft[2 * v + 1];
     double gtc = 0.0;

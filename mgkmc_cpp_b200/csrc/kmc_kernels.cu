@@ -15,6 +15,7 @@
 //             464-564 / :1413-1422, 1473-1590): the first entry per voxel of the
 //             Q-sorted unstable list is that voxel's lowest-Q unstable mode, and
 //             the flips run in the order of those Q values.
+#include <algorithm>
 #include "kmc_kernels.cuh"
 #include "kmc_device.cuh"
 
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(512) select_flip_kernel(KmcDevState s, KmcPhys
         st->selected = k;
         st->is_instab = s.Q[k] <= p.threshold ? 1 : 0;
         st->margin = s_margin;
-        apply_flip<D, C>(s, p, k, time, nullptr);
+        apply_flip<D, C>(s, p, k, time, s.flipcat);
     }
     __syncthreads();
     redraw<C>(s, k, draws, redraw_dir, redraw_bar, threadIdx.x, blockDim.x);
@@ -313,7 +314,7 @@ __global__ void cascade_apply_kernel(KmcDevState s, KmcPhys p, const int* modes,
         if (blockIdx.x != 0) return;
         for (int f = 0; f < n; ++f) {
             const long k = modes[f];
-            if (threadIdx.x == 0) apply_flip<D, C>(s, p, k, time, nullptr);
+            if (threadIdx.x == 0) apply_flip<D, C>(s, p, k, time, s.flipcat ? s.flipcat + (long)f * C : nullptr);
             __syncthreads();
             redraw<C>(s, k, draws + (long)f * rec * (C + 1), redraw_dir, redraw_bar, threadIdx.x, blockDim.x);
             __syncthreads();
@@ -322,12 +323,112 @@ __global__ void cascade_apply_kernel(KmcDevState s, KmcPhys p, const int* modes,
     }
     for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < n; f += (long)gridDim.x * blockDim.x) {
         const long k = modes[f];
-        apply_flip<D, C>(s, p, k, time, nullptr);
+        apply_flip<D, C>(s, p, k, time, s.flipcat ? s.flipcat + f * C : nullptr);
         redraw<C>(s, k, draws + f * rec * (C + 1), redraw_dir, redraw_bar, 0, 1);
     }
 }
 
+template <int D>
+__global__ void stress_kernel(KmcDevState s) {
+    constexpr int S = D == 2 ? 3 : 6;
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < s.N; v += (long)gridDim.x * blockDim.x) {
+        double sg[S];
+        voxel_stress<D>(s, (int)v, sg);
+#pragma unroll
+        for (int c = 0; c < S; ++c) s.sig_s[(long)c * s.N + v] = sg[c];
+    }
+}
+
+// Coefficients of a mode on the stress-kernel bases: 2D {xx = -yy, xy}
+// (kmc_solver.hpp:884-885); 3D {diag(1,-1,0), diag(0,1,-1), xy, xz, yz} with
+// c0 = C(0,0), c1 = -C(2,2), c2..c4 = C(0,1), C(0,2), C(1,2) (:1895-1899).
+template <int D, int C>
+MGK_DEV int basis_coef(const double* cat, double* coef) {
+    constexpr int S = D == 2 ? 3 : 6;
+    double cs[S];
+    cat_sym<D, C>(cat, cs);
+    if (D == 2) {
+        coef[0] = cs[0];
+        coef[1] = cs[2];
+        return 2;
+    }
+    coef[0] = cs[0];
+    coef[1] = -cs[2];
+    coef[2] = cs[3];
+    coef[3] = cs[4];
+    coef[4] = cs[5];
+    return 5;
+}
+
+// One thread per voxel: the voxel's own additions in the reference's order
+// (predictor; per flip: every stencil offset that lands on the voxel, in
+// dx, dy, dz loop order, then the missing mean), with explicit
+// round-to-nearest operations so that no multiply-add is contracted.
+template <int D, int C>
+__global__ void patch_kernel(KmcDevState s, KmcPhys p, const int* modes, int nflips, const double* K, const double* miss,
+                             int R, const double* unit, double pred) {
+    constexpr int S = D == 2 ? 3 : 6;
+    const int nx = p.nx, ny = p.ny, nz = D == 3 ? p.nz : 1;
+    const int side = 2 * R + 1, side_z = (D == 3 && nz > 1) ? side : 1;
+    const int P = side * side * side_z;
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < s.N; v += (long)gridDim.x * blockDim.x) {
+        const int vx = (int)(v / ((long)ny * nz)), vy = (int)((v / nz) % ny), vz = (int)(v % nz);
+        double val[S];
+#pragma unroll
+        for (int c = 0; c < S; ++c) val[c] = s.sig_s[(long)c * s.N + v];
+        if (pred != 0.0)
+#pragma unroll
+            for (int c = 0; c < S; ++c) val[c] = __dadd_rn(val[c], __dmul_rn(unit[c], pred));
+        for (int f = 0; f < nflips; ++f) {
+            const long k = modes[f];
+            const int u = (int)(k / s.M);
+            const int x = u / (ny * nz), y = (u / nz) % ny, z = u % nz;
+            double coef[5];
+            const int nb = basis_coef<D, C>(s.flipcat + (long)f * C, coef);
+            // offsets d in [-R, R] with (x + d) mod n == vx, ascending
+            const int ddx = ((vx - x) % nx + nx) % nx, ddy = ((vy - y) % ny + ny) % ny, ddz = ((vz - z) % nz + nz) % nz;
+            for (int dx = ddx - nx * ((ddx + R) / nx); dx <= R; dx += nx)
+                for (int dy = ddy - ny * ((ddy + R) / ny); dy <= R; dy += ny) {
+                    const int z0 = side_z > 1 ? ddz - nz * ((ddz + R) / nz) : 0, z1 = side_z > 1 ? R : 0;
+                    for (int dz = z0; dz <= z1; dz += (side_z > 1 ? nz : 1)) {
+                        const int crop = ((dx + R) * side + (dy + R)) * side_z + (side_z > 1 ? dz + R : 0);
+#pragma unroll
+                        for (int c = 0; c < S; ++c) {
+                            double pv = __dmul_rn(coef[0], K[(long)crop * S + c]);
+                            for (int b = 1; b < nb; ++b) pv = __dadd_rn(pv, __dmul_rn(coef[b], K[((long)b * P + crop) * S + c]));
+                            val[c] = __dadd_rn(val[c], pv);
+                        }
+                    }
+                }
+#pragma unroll
+            for (int c = 0; c < S; ++c) {
+                double ms = __dmul_rn(coef[0], miss[c]);
+                for (int b = 1; b < nb; ++b) ms = __dadd_rn(ms, __dmul_rn(coef[b], miss[b * S + c]));
+                val[c] = __dadd_rn(val[c], ms);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < S; ++c) s.sig_s[(long)c * s.N + v] = val[c];
+    }
+}
+
 }  // namespace
+
+cudaError_t kmc_stress(const KmcDevState& s, cudaStream_t st) {
+    const int grid = (int)std::min<long>((s.N + 255) / 256, 148 * 8);
+    if (s.D == 2) stress_kernel<2><<<grid, 256, 0, st>>>(s);
+    else stress_kernel<3><<<grid, 256, 0, st>>>(s);
+    return cudaGetLastError();
+}
+
+cudaError_t kmc_patch(const KmcDevState& s, const KmcPhys& p, const int* modes, int nflips, const double* K,
+                      const double* miss, int R, const double* unit, double pred, cudaStream_t st) {
+    const int grid = (int)std::min<long>((s.N + 255) / 256, 148 * 8);
+    if (s.D == 2) patch_kernel<2, 2><<<grid, 256, 0, st>>>(s, p, modes, nflips, K, miss, R, unit, pred);
+    else if (s.C == 2) patch_kernel<3, 2><<<grid, 256, 0, st>>>(s, p, modes, nflips, K, miss, R, unit, pred);
+    else patch_kernel<3, 6><<<grid, 256, 0, st>>>(s, p, modes, nflips, K, miss, R, unit, pred);
+    return cudaGetLastError();
+}
 
 int kmc_sweep_blocks(long NM, int items) {
     const long per = (long)kSweepThreads * items;

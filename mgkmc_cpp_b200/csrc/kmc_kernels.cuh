@@ -23,6 +23,11 @@ struct KmcDevState {
     const double* eps_s;  // S * N (owned by the LS solver)
     const double* lam;    // N
     const double* mu;     // N
+    // fast patching only (else null): the stress field the sweep reads
+    // (kept by stencil updates between LS solves) and, per flip of the last
+    // select / cascade batch, the flipped mode's catalog entry before its redraw
+    double* sig_s;        // S * N
+    double* flipcat;      // N * C
 };
 
 struct KmcPhys {
@@ -70,5 +75,15 @@ cudaError_t kmc_cascade_collect(const KmcDevState& s, const KmcPhys& p, double* 
 cudaError_t kmc_cascade_flip(const KmcDevState& s, const KmcPhys& p, double* keys, int* modes, int n, double* tmp_keys,
                              int* tmp_modes, double time, const double* draws, int redraw_dir, int redraw_bar,
                              KmcStatus* status, cudaStream_t st);
+
+// Fast patching (kmc_solver.hpp:276-332, 866-913, 525-546, 942-947):
+// sig_s = stress of the current LS strain field (after every LS solve).
+cudaError_t kmc_stress(const KmcDevState& s, cudaStream_t st);
+// sig_s += unit * pred (when pred != 0), then for every flip f in order (flat
+// mode modes[f], pre-redraw catalog flipcat[f]): the stencil of the stress
+// kernels K (nb bases, side^D... entries of S values each) around the flipped
+// voxel weighted by the mode's basis coefficients, then the missing mean.
+cudaError_t kmc_patch(const KmcDevState& s, const KmcPhys& p, const int* modes, int nflips, const double* K,
+                      const double* miss, int R, const double* unit, double pred, cudaStream_t st);
 
 }  // namespace mgk

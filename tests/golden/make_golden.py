@@ -268,9 +268,84 @@ def main_le():
         print("wrote", name, glog.count("\n"), "global-log lines")
 
 
+# fast patching (kmc_solver.hpp:276-332, 866-913): the reference's own
+# run_simulation (ref_driver kmc_run) over a short loading with thermal
+# events, cascades and periodic full solves; its final state and summary log
+FP_YAML = """seed: {seed}
+system:
+  dimensionality: "{dim}"
+  plane_mode: "plane_strain"
+  nx: {nx}
+  ny: {ny}
+  nz: {nz}
+  pixel: 1.0
+  M: {M}
+  gamma0: {g0}
+  3d_barriers: {b3}
+material:
+  E:
+    mode: "constant"
+    value: 90
+  nu:
+    mode: "constant"
+    value: 0.36
+loading:
+  eps_target: 2e-5
+  step_size: 1e-6
+boundary_conditions:
+  driving_component: "{drive}"
+  mixed_targets:
+{targets}
+  mixed_tol: 1.0
+barriers:
+  type: "gaussian"
+  kwargs:
+    mean: 2.0
+    std: 0.6
+    min_cutoff: 0.1
+physics:
+  enable_softening: true
+  softening_scheme: "isotropic"
+  jp: 1.0
+  jt: 3.0
+  softening_cap: 0.5
+dynamics:
+  instability_mode: "cascade"
+  temperature: 300
+  nu0: 1e13
+  physical_strain_rate: 0.1
+  fast_patching:
+    enabled: true
+    patch_radius: {R}
+    sync_interval: {sync}
+"""
+FP_CASES = {
+    "fp2d_16": dict(seed=5, dim="2d", nx=16, ny=16, nz=1, M=6, g0=0.1, b3="false", drive="xx",
+                    targets="    yy: 0.0\n    xy: 0.0", R=3, sync=4, nsteps=20),
+    "fp3d_8x8x6": dict(seed=9, dim="3d", nx=8, ny=8, nz=6, M=8, g0=0.05, b3="true", drive="zz",
+                       targets="    xx: 0.0\n    yy: 0.0", R=2, sync=3, nsteps=20),
+}
+
+
+def main_fp():
+    rd = O.RefDriver()
+    for name, c in FP_CASES.items():
+        y = FP_YAML.format(**c)
+        res = rd.kmc(y, "kmc_run", nsteps=c["nsteps"])
+        arrs = {f: res[f] for f in ("eps", "sig", "epsp", "catalog", "Q0", "soft", "macro")}
+        arrs["yaml"] = np.array(y)
+        arrs["summary"] = np.array(res["summary"])
+        arrs["nsteps"] = np.array(c["nsteps"])
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
+        print("wrote", name, res["summary"].count("KMC"), "KMC rows,", res["summary"].count("CASCADE"), "cascade rows")
+
+
 if __name__ == "__main__":
     if "--le" in sys.argv:
         main_le()
+    elif "--fp" in sys.argv:
+        main_fp()
     else:
         main()
         main_le()
+        main_fp()

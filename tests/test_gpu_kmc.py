@@ -89,8 +89,9 @@ def test_kmc_logs_and_vtu(G, tmp_path):
     assert 'NumberOfPoints="338" NumberOfCells="144"' in txt and "eps_plastic_vm" in txt and "g_t" in txt
 
 
-def test_kmc_unsupported_and_bad_args(G):
-    with pytest.raises(G.MgkError, match="UNSUPPORTED"):
-        G.KmcSimulation2D(4, 4, 2, 0.1, np.full(16, 90e9), np.full(16, 0.3), fast_patching_enabled=True)
+def test_kmc_bad_args(G):
+    with pytest.raises(G.MgkError, match="BAD_SHAPE"):
+        G.KmcSimulation2D(4, 4, 2, 0.1, np.full(16, 90e9), np.full(16, 0.3), fast_patching_enabled=True,
+                          sync_interval=0)
     with pytest.raises(ValueError):
         G.KmcSimulation2D(4, 4, 2, 0.1, np.full(15, 90e9), np.full(16, 0.3))

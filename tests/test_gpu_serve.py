@@ -63,6 +63,28 @@ def test_served_job_same_alone_and_in_mix(G, tmp_path):
     assert len(srv.step_latency_us) == sum(srv.done[j]["events"] for j in srv.done)
 
 
+def test_time_sliced_serving_same_as_alone(G, tmp_path):
+    """Time slices (the default): every job stops at its first decision past
+    the slice's device time; the flips are still exactly the job's own."""
+    cfgs = [_cfg("ens2d_64", 3, tmp_path), _cfg("ens2d_128", 1, tmp_path), _cfg("hetero3d_16", 1, tmp_path)]
+    targets = [150, 80, 40]
+    refs = []
+    for c, t in zip(cfgs, targets):
+        b = G.KmcBatch([c])
+        b.run(t)
+        refs.append(b.stats(0)["selected"])
+        b.close()
+    srv = G.Server(slice_seconds=0.002)
+    ids = [srv.submit(c, t, arrival=float(i)) for i, (c, t) in enumerate(zip(cfgs, targets))]
+    now = 0.0
+    while not srv.idle():
+        srv.step(now)
+        now += 1.0
+    assert srv.launches > 3
+    for jid, ref in zip(ids, refs):
+        assert np.array_equal(srv.done[jid]["selected"], ref)
+
+
 def test_admission_gated_by_free_memory(G, tmp_path):
     """With an HBM budget that holds one job, jobs run one at a time."""
     cfgs = [_cfg("ens2d_64", s, tmp_path) for s in range(3)]
