@@ -300,7 +300,7 @@ def main():
     ap.add_argument("--cpu-events", type=int, default=40, help="events per replica in the bounded CPU-baseline sample")
     ap.add_argument("--ref-events", type=int, default=150, help="events per replica timed by --impl reference")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-replica ensemble block")
-    ap.add_argument("--ensemble-seconds", type=float, default=10.0)
+    ap.add_argument("--ensemble-seconds", type=float, default=20.0)
     ap.add_argument("--serve-jobs", type=int, default=40, help="jobs of the serving block (0: skip)")
     ap.add_argument("--serve-flips", type=int, nargs=2, default=[50, 500])
     ap.add_argument("--serve-full-sizes", action="store_true",

@@ -152,7 +152,7 @@ MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
     dd acc = {0.0, 0.0};
     int unst = 0, last = -1;
     // four tiles per warp and pass: independent exp / reduction chains in
-    // flight (one CTA per SM leaves only 8 warps to hide latency)
+    // flight (two 256-thread CTAs per SM leave only 16 warps to hide latency)
     constexpr int U = 4;
     for (long tb = wid; tb < ntile; tb += (long)nw * U) {
         dd r[U];
@@ -899,7 +899,7 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
     }
 }
 
-__global__ void __launch_bounds__(256, 1) batch_kernel(BatchRep* reps, const int2* map, size_t smem_bytes) {
+__global__ void __launch_bounds__(256, 2) batch_kernel(BatchRep* reps, const int2* map, size_t smem_bytes) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int2 m = map[blockIdx.x];
     BatchRep& R = reps[m.x];
@@ -990,30 +990,51 @@ void BatchEngine::init() {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    // one CTA per SM (the kernel needs ~250 registers a thread); the dynamic
-    // shared memory holds two LS FFT buffers (or the cascade sort / redraw
-    // scratch) and, past them, the replica generator
-    const int per_sm = 1;
-    const size_t half_budget = 92 * 1024;
+    // two CTAs per SM: 128 registers a thread (the kernel spills ~2 kB a
+    // thread at that bound, and still runs 12-37 % faster than one 254-register
+    // CTA per SM, measured on B200); the dynamic shared memory of each holds
+    // two LS FFT buffers (or the cascade sort / redraw scratch) and, past
+    // them, the replica generator
+    const int per_sm = 2;
+    const size_t half_budget = 36 * 1024;
     const int budget = per_sm * nsm;
     if (n > budget) throw std::invalid_argument("more replicas than co-resident CTAs");
-    // CTA groups: every replica gets one CTA, then each further CTA goes to
-    // the replica whose event rate it raises most, by the model
+    // CTA groups: every replica gets its floor (below), then each further CTA
+    // goes to the replica whose event rate it raises most, by the model
     // t_event(c) = kSecPerWork * work / c + kSecPerEvent (work = modes swept +
-    // 24 x LS voxels; the constants are fitted to measured 64^2 runs on one
-    // and nine CTAs).  This maximises the batch's total steps/s: small grids,
+    // 24 x LS voxels in 2D, 72 x in 3D; the constants are fitted to measured
+    // 64^2 runs on one and nine CTAs).  This maximises the batch's total steps/s: small grids,
     // whose events are latency-bound, gain most from extra CTAs; the largest
     // grids still advance on the CTAs their share of the model gives them.
     constexpr double kSecPerWork = 12.7e-9, kSecPerEvent = 160e-6;
     std::vector<double> work(n);
     std::vector<int> lim(n);
     for (int r = 0; r < n; ++r) {
-        work[r] = (double)eng_[r]->NM_ + 24.0 * eng_[r]->N_;
+        // a 3D LS voxel costs ~3x a 2D one (6 components, 3 FFT axes; measured
+        // 32^3 events against the 2D fit)
+        work[r] = (double)eng_[r]->NM_ + (eng_[r]->D_ == 2 ? 24.0 : 72.0) * eng_[r]->N_;
         lim[r] = std::max(1, std::min(eng_[r]->ls_->grid_, 160));
     }
     auto rate = [&](int r, int c) { return 1.0 / (kSecPerWork * work[r] / c + kSecPerEvent); };
+    // floor: enough CTAs that a replica's modelled event time stays under
+    // kMaxEventSeconds (a large grid on one CTA would otherwise take seconds
+    // per event, and a run or a serving slice waits for its last event)
+    constexpr double kMaxEventSeconds = 0.25;
     ncta_.assign(n, 1);
-    int used = n;
+    int used = 0;
+    for (int r = 0; r < n; ++r) {
+        const int need = (int)std::ceil(kSecPerWork * work[r] / (kMaxEventSeconds - kSecPerEvent));
+        ncta_[r] = std::max(1, std::min(lim[r], need));
+        used += ncta_[r];
+    }
+    while (used > budget) {  // the floors do not fit: take from the largest groups
+        int big = 0;
+        for (int r = 1; r < n; ++r)
+            if (ncta_[r] > ncta_[big]) big = r;
+        if (ncta_[big] <= 1) break;
+        --ncta_[big];
+        --used;
+    }
     while (used < budget) {
         int best = -1;
         double gain = 0.0;
