@@ -159,6 +159,17 @@ MGK_API mgk_status mgk_kmc_get_field(mgk_kmc* h, int field, double* dst, long lo
 MGK_API mgk_status mgk_kmc_get_macro(mgk_kmc* h, double* out, int n);
 MGK_API void mgk_kmc_destroy(mgk_kmc* h);
 
+/* ---------------------------------------------------------------- generated material fields
+ * generate_correlated_field_cpp (material_generator.hpp:130-258, main.cpp's
+ * "generated" material mode) on the GPU: N = nx*ny(*nz) values into out (host)
+ * -- Box-Muller normals from std::mt19937(seed), an orthonormal FFT, the
+ * Gaussian filter exp(-2 pi^2 corr^2 |f|^2), the inverse FFT, standardisation,
+ * then mean + std * g clipped to [clip_min, clip_max] where enabled.  Axis
+ * lengths must factor into 2, 3, 5 and 7 (MGK_BAD_SHAPE otherwise). */
+MGK_API mgk_status mgk_correlated_field(int dim, int nx, int ny, int nz, double mean, double std_dev, double corr,
+                                        int has_min, double clip_min, int has_max, double clip_max, int seed,
+                                        double* out);
+
 /* ---------------------------------------------------------------- linear-elastic simulation
  * Replaces main.cpp's simulation_type "linear_elastic" branch
  * (main.cpp:418-869): the macroscopic target (eps_target on the driving

@@ -387,6 +387,21 @@ def run_config(path_or_cfg, output_dir: Optional[str] = None):
     return sim
 
 
+def correlated_field_gpu(shape, mean: float, std: float, corr: float, seed: int, clip_min=None, clip_max=None):
+    """generate_correlated_field_cpp (material_generator.hpp:130-258) on the
+    GPU; same arguments as fields.correlated_field."""
+    shape = tuple(int(s) for s in shape)
+    dim = len(shape)
+    nx, ny = shape[0], shape[1]
+    nz = shape[2] if dim == 3 else 1
+    out = np.zeros(int(np.prod(shape)))
+    _lib.check(_lib.lib().mgk_correlated_field(dim, nx, ny, nz, float(mean), float(std), float(corr),
+                                               int(clip_min is not None), float(clip_min or 0.0),
+                                               int(clip_max is not None), float(clip_max or 0.0), int(seed),
+                                               _lib.dptr(out)))
+    return out.reshape(shape)
+
+
 def device_memory():
     """(free, total) bytes of the current device."""
     f, t = _lib.C.c_ulonglong(0), _lib.C.c_ulonglong(0)

@@ -21,7 +21,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmgkmc_b200.so")
 CLI = os.path.join(HERE, "mgkmc_b200")
 
-SOURCES = ["ls.cu", "kmc_kernels.cu", "engine.cu", "batch.cu", "elastic.cu", "capi.cu", "vtu.cpp"]
+SOURCES = ["ls.cu", "kmc_kernels.cu", "engine.cu", "batch.cu", "elastic.cu", "fieldgen.cu", "capi.cu", "vtu.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_FLAGS = "-fPIC,-O2,-ffp-contract=off,-fvisibility=hidden"
 

@@ -8,6 +8,7 @@
 #include "../../include/mgkmc_b200.h"
 #include "batch.cuh"
 #include "elastic.cuh"
+#include "fieldgen.cuh"
 #include "engine.cuh"
 #include "ls.cuh"
 
@@ -208,6 +209,20 @@ mgk_status mgk_kmc_get_profile(mgk_kmc* h, double* out, double* lat, long long l
     std::memcpy(out, v, sizeof(v));
     if (lat)
         for (long long i = 0; i < lat_cap && i < (long long)p.event_us.size(); ++i) lat[i] = p.event_us[i];
+    return MGK_OK;
+}
+
+mgk_status mgk_correlated_field(int dim, int nx, int ny, int nz, double mean, double std_dev, double corr, int has_min,
+                                double clip_min, int has_max, double clip_max, int seed, double* out) {
+    if (!out) return fail(MGK_BAD_ARG, "null output");
+    if (dim != 2 && dim != 3) return fail(MGK_BAD_ARG, "dim must be 2 or 3");
+    if (nx < 1 || ny < 1 || (dim == 3 && nz < 1)) return fail(MGK_BAD_SHAPE, "bad grid");
+    try {
+        mgk::correlated_field(dim, nx, ny, nz, mean, std_dev, corr, has_min != 0, clip_min, has_max != 0, clip_max, seed,
+                              out);
+    } catch (const std::exception& e) {
+        return from_exception(e);
+    }
     return MGK_OK;
 }
 

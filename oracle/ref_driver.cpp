@@ -486,13 +486,30 @@ static int cmd_draws(int seed, int n, const std::string& out) {
     return 0;
 }
 
+// generate_correlated_field_cpp (material_generator.hpp:130-258), as main.cpp's
+// "generated" material mode calls it: the field of NX x NY x NZ voxels.
+static int cmd_grf(char** a, const std::string& out) {
+    const int nx = atoi(a[0]), ny = atoi(a[1]), nz = atoi(a[2]), is3d = atoi(a[3]);
+    const double mean = atof(a[4]), sd = atof(a[5]), corr = atof(a[6]);
+    const int has_min = atoi(a[7]);
+    const double cmin = atof(a[8]);
+    const int has_max = atoi(a[9]);
+    const double cmax = atof(a[10]);
+    const int seed = atoi(a[11]);
+    std::vector<double> f = generate_correlated_field_cpp(nx, ny, nz, is3d != 0, mean, sd, corr, has_min != 0, cmin,
+                                                          has_max != 0, cmax, seed);
+    write_npy(out, f, {f.size()});
+    return 0;
+}
+
 int main(int argc, char** argv) {
-    if (argc < 3) { std::cerr << "usage: ref_driver ls2d|ls3d DIR | kmc_run CFG OUT NSTEPS | kmc_trace CFG OUT NSTEPS MAXEV | kmc_init CFG OUT | draws SEED N OUT\n"; return 2; }
+    if (argc < 3) { std::cerr << "usage: ref_driver ls2d|ls3d DIR | kmc_run CFG OUT NSTEPS | kmc_trace CFG OUT NSTEPS MAXEV | kmc_init CFG OUT | draws SEED N OUT | grf NX NY NZ IS3D MEAN STD CORR HASMIN MIN HASMAX MAX SEED OUT\n"; return 2; }
     std::string cmd = argv[1];
     try {
         if (cmd == "ls2d") return cmd_ls2d(argv[2]);
         if (cmd == "ls3d") return cmd_ls3d(argv[2]);
         if (cmd == "draws" && argc >= 5) return cmd_draws(atoi(argv[2]), atoi(argv[3]), argv[4]);
+        if (cmd == "grf" && argc >= 15) return cmd_grf(argv + 2, argv[14]);
         if ((cmd == "kmc_run" || cmd == "kmc_trace" || cmd == "kmc_init") && argc >= 4) {
             RunCfg r = load_cfg(argv[2]);
             std::string out = argv[3];

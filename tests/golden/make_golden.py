@@ -340,8 +340,34 @@ def main_fp():
         print("wrote", name, res["summary"].count("KMC"), "KMC rows,", res["summary"].count("CASCADE"), "cascade rows")
 
 
+# generate_correlated_field_cpp (material_generator.hpp:130-258), the
+# reference's own output for main.cpp's "generated" material mode
+GRF_CASES = {
+    "grf2d_32x24": dict(nx=32, ny=24, nz=1, is3d=0, mean=70.0, std=7.0, corr=4.0, has_min=1, cmin=55.0, has_max=0,
+                        cmax=0.0, seed=11),
+    "grf3d_12x10x8": dict(nx=12, ny=10, nz=8, is3d=1, mean=90.0, std=9.0, corr=3.0, has_min=0, cmin=0.0, has_max=1,
+                          cmax=100.0, seed=5),
+}
+
+
+def main_grf():
+    rd = O.RefDriver()
+    for name, c in GRF_CASES.items():
+        with tempfile.TemporaryDirectory() as d:
+            out = os.path.join(d, "f.npy")
+            args = [c[k] for k in ("nx", "ny", "nz", "is3d", "mean", "std", "corr", "has_min", "cmin", "has_max", "cmax",
+                                   "seed")]
+            subprocess.run([rd.path, "grf"] + [repr(a) if isinstance(a, float) else str(a) for a in args] + [out],
+                           check=True, capture_output=True)
+            f = np.load(out)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), field=f, **{k: np.array(v) for k, v in c.items()})
+        print("wrote", name, f.shape, float(f.mean()), float(f.std()))
+
+
 if __name__ == "__main__":
-    if "--le" in sys.argv:
+    if "--grf" in sys.argv:
+        main_grf()
+    elif "--le" in sys.argv:
         main_le()
     elif "--fp" in sys.argv:
         main_fp()
@@ -349,3 +375,4 @@ if __name__ == "__main__":
         main()
         main_le()
         main_fp()
+        main_grf()

@@ -52,3 +52,19 @@ def test_box_muller_stream_is_std_mt19937():
     r = bg.random_raw(2).astype(np.float64) / 4294967296.0
     want = np.sqrt(-2 * np.log(r[0])) * np.cos(2 * np.pi * r[1])
     assert fields.box_muller_normals(1, 5)[0] == want
+
+
+def test_correlated_field_matches_reference():
+    """fields.correlated_field against generate_correlated_field_cpp itself
+    (golden grf*.npz from the reference sources): same MT19937 stream and
+    Box-Muller draws, an FFT of another library, so within 1e-12."""
+    from helpers import golden
+    from mgkmc_cpp_b200 import fields
+    for name in ("grf2d_32x24", "grf3d_12x10x8"):
+        g = golden(name)
+        shape = (int(g["nx"]), int(g["ny"])) + ((int(g["nz"]),) if int(g["is3d"]) else ())
+        f = fields.correlated_field(shape, float(g["mean"]), float(g["std"]), float(g["corr"]), int(g["seed"]),
+                                    clip_min=float(g["cmin"]) if int(g["has_min"]) else None,
+                                    clip_max=float(g["cmax"]) if int(g["has_max"]) else None)
+        ref = g["field"].reshape(shape)
+        assert np.max(np.abs(f - ref)) <= 1e-12 * np.max(np.abs(ref)), name
