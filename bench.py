@@ -254,6 +254,51 @@ def ensemble_block(G, workloads, workdir, seconds, plain_events):
             "per_class": classes, "setup_seconds": t_setup}
 
 
+# algorithmic bytes of one LS iteration per voxel with an FP32 spectrum: the
+# FP64 real-space traffic and S complex FP32 words written and read once
+BYTES_LS_FP32 = {2: 8 * (3 * 3 + 2) + 2 * 3 * 8 // 2, 3: 8 * (3 * 6 + 2) + 2 * 6 * 8 // 2}
+
+
+def precision_block(G, cases=(((512, 512), 11), ((64, 64, 64), 12)), solves=3):
+    """The precision form of the LS solve: FP64 against FP32-refined (FP32
+    spectrum and FFTs to a relative change of 1e-6, then FP64 iterations), on
+    a lognormal modulus field (CoV 0.1), cold starts at the reference's
+    tolerance (1e-6) timed on the device, and the two fields compared after
+    both are solved to 1e-11."""
+    from mgkmc_cpp_b200 import fields
+    out = {}
+    for dims, seed in cases:
+        D = len(dims)
+        N = int(np.prod(dims))
+        E = fields.lognormal_modulus(dims, 90e9, 0.10, 4.0 if D == 2 else 3.0, seed).reshape(-1)
+        nu = np.full(N, 0.36)
+        eb = np.zeros((D, D))
+        eb[0, 0], eb[1, 1], eb[0, 1], eb[1, 0] = 1e-3, -4e-4, 2e-4, 2e-4
+        row, fields_at = {}, {}
+        for prec in ("fp64", "fp32_refined"):
+            s = G.LsSolver(dims, E, nu, precision=prec)
+            s.solve(eb, tol=1e-6)
+            ms, its = [], []
+            for _ in range(solves):
+                r = s.solve(eb, tol=1e-6)
+                ms.append(s.last_solve_ms())
+                its.append(r[4])
+            fields_at[prec] = s.solve(eb, tol=1e-11, max_iter=1000)[0]
+            s.close()
+            t = float(np.median(ms))
+            it = float(np.median(its))
+            per_voxel = BYTES_LS[D] if prec == "fp64" else BYTES_LS_FP32[D]
+            row[prec] = {"ms_per_solve": t, "iterations": it, "ls_voxel_iterations_per_s": N * it / (t / 1e3),
+                         "achieved_gbs": per_voxel * N * it / (t / 1e3) / 1e9}
+        e64, e32 = fields_at["fp64"], fields_at["fp32_refined"]
+        row["field_rel_l2_fp32_refined_vs_fp64_at_tol_1e-11"] = float(np.linalg.norm(e32 - e64) / np.linalg.norm(e64))
+        row["speedup"] = row["fp64"]["ms_per_solve"] / row["fp32_refined"]["ms_per_solve"]
+        out["x".join(map(str, dims))] = row
+        progress("precision: %s fp64 %.3f ms, fp32-refined %.3f ms" % (dims, row["fp64"]["ms_per_solve"],
+                                                                       row["fp32_refined"]["ms_per_solve"]))
+    return out
+
+
 def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05):
     """The serving loop on a Poisson request stream (20 jobs/s, seed 7): jobs
     are admitted as they arrive (wall clock) and as memory allows, every
@@ -300,6 +345,9 @@ def main():
     ap.add_argument("--cpu-events", type=int, default=40, help="events per replica in the bounded CPU-baseline sample")
     ap.add_argument("--ref-events", type=int, default=150, help="events per replica timed by --impl reference")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-replica ensemble block")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP64 / FP32-refined LS block")
+    ap.add_argument("--only-precision", action="store_true",
+                    help="run only the FP64 / FP32-refined LS block and print its JSON (profiling the LS kernels)")
     ap.add_argument("--ensemble-seconds", type=float, default=20.0)
     ap.add_argument("--serve-jobs", type=int, default=40, help="jobs of the serving block (0: skip)")
     ap.add_argument("--serve-flips", type=int, nargs=2, default=[50, 500])
@@ -352,6 +400,10 @@ def main():
 
     # ------------------------------------------------------------------ b200 arm
     import mgkmc_cpp_b200 as G
+
+    if args.only_precision:
+        print(json.dumps({"precision": precision_block(G)}))
+        return 0
 
     dist, dev = None, None
     if world > 1:
@@ -441,6 +493,12 @@ def main():
             ens = ensemble_block(G, workloads, workdir, args.ensemble_seconds, 20)
         except Exception as e:  # reported, never silently dropped
             ens = {"error": str(e)[-300:]}
+    prec = None
+    if rank == 0 and not args.no_precision:
+        try:
+            prec = precision_block(G)
+        except Exception as e:
+            prec = {"error": str(e)[-300:]}
     srv = None
     progress("serving")
     if args.serve_jobs > 0 and rank == 0:
@@ -496,6 +554,8 @@ def main():
         line["ensemble"] = ens
     if srv is not None:
         line["serving"] = srv
+    if prec is not None:
+        line["precision"] = prec
     if args.gpus == 1:
         progress("cpu baseline")
         res, err = run_reference(cfg_paths, args.cpu_events)

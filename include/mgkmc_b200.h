@@ -64,6 +64,16 @@ MGK_API mgk_status mgk_ls_create(mgk_ls** out, int dim, int nx, int ny, int nz, 
  * loop hit max_iter (fields are still written, like the reference). */
 MGK_API mgk_status mgk_ls_solve(mgk_ls* h, const double* eps_bar, const double* eps_plastic, double* eps_inout, int warm,
                         double* sig_out, double* macro_out, int max_iter, double tol, int* iters_out);
+/* Precision of later solves (no counterpart in the reference, which is FP64):
+ * 0 FP64 (default); 1 FP32-refined -- FP32 spectrum, FFTs and Green operator
+ * (real-space strain, polarisation, norms and macro sums stay FP64) until the
+ * relative change is below max(tol, 1e-6), then FP64 iterations from that
+ * field to tol; each phase is capped at max_iter and iters_out reports their
+ * sum. */
+MGK_API mgk_status mgk_ls_set_precision(mgk_ls* h, int precision);
+/* Device time (ms, CUDA events on the solver's stream) of the last solve's
+ * kernel launches, without its host copies. */
+MGK_API mgk_status mgk_ls_last_solve_ms(mgk_ls* h, double* ms);
 MGK_API void mgk_ls_destroy(mgk_ls* h);
 
 /* ---------------------------------------------------------------- LS solve without allocating

@@ -54,7 +54,9 @@ def _as_tensors(a, N: int, D: int) -> np.ndarray:
 class LsSolver:
     """Device-resident Lippmann-Schwinger solver for one grid and modulus field."""
 
-    def __init__(self, dims, E, nu, plane_mode: str = "plane_strain", pixel: float = 1.0):
+    def __init__(self, dims, E, nu, plane_mode: str = "plane_strain", pixel: float = 1.0, precision: str = "fp64"):
+        """precision: "fp64" (the reference's arithmetic) or "fp32_refined" (FP32
+        spectrum and FFTs to a relative change of 1e-6, then FP64 iterations)."""
         L = _lib.lib()
         _lib.require_device()
         self.dims = tuple(int(d) for d in dims)
@@ -72,6 +74,15 @@ class LsSolver:
                                    1 if plane_mode == "plane_stress" else 0, float(pixel), _lib.dptr(self._E),
                                    _lib.dptr(self._nu)))
         self._h = h
+        if precision not in ("fp64", "fp32_refined"):
+            raise ValueError("precision must be 'fp64' or 'fp32_refined'")
+        _lib.check(L.mgk_ls_set_precision(h, 1 if precision == "fp32_refined" else 0))
+
+    def last_solve_ms(self) -> float:
+        """Device time of the last solve's kernels (no host copies)."""
+        ms = np.zeros(1)
+        _lib.check(_lib.lib().mgk_ls_last_solve_ms(self._h, _lib.dptr(ms)))
+        return float(ms[0])
 
     def solve(self, eps_bar, eps=None, eps_plastic=None, max_iter: int = 200, tol: float = 1e-6):
         """Returns (eps, sig, eps_macro, sig_macro, iterations); ``eps`` given = warm start."""
@@ -503,9 +514,9 @@ class Server:
             job["selected"].append(st["selected"])
             job["latency_us"].extend(st["event_us"].tolist())
             self.step_latency_us.extend(st["event_us"].tolist())
-            # a job without an event for stall_seconds of device time (a
-            # cascade that does not settle) is retired as stalled
-            job["idle_s"] = job["idle_s"] + ms / 1e3 if st["events"] == 0 else 0.0
+            # a job without a decision (a sweep) for stall_seconds of device
+            # time is retired as stalled; cascade batches count as progress
+            job["idle_s"] = job["idle_s"] + ms / 1e3 if st["sweeps"] == 0 else 0.0
             job["stalled"] = job["idle_s"] >= self.stall_seconds
             if job["events"] >= job["target"] or st["terminated"] == 1 or job["stalled"]:
                 job["finished"] = now

@@ -15,6 +15,7 @@
 // initial draws is handed to the device and continued by one thread with the
 // reference's distributions (mt_device.cuh), so the draws follow the
 // reference's stream; only device log/exp may differ from glibc by an ulp.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <thread>
@@ -995,8 +996,17 @@ void BatchEngine::init() {
     // CTA per SM, measured on B200); the dynamic shared memory of each holds
     // two LS FFT buffers (or the cascade sort / redraw scratch) and, past
     // them, the replica generator
-    const int per_sm = 2;
     const size_t half_budget = 36 * 1024;
+    // CTAs per SM: two when the largest launch this plan can make fits twice
+    int per_sm = 0;
+    {
+        const size_t smem_max = std::max({(size_t)4096 * 12, kRedrawSmem, 2 * half_budget}) + sizeof(rng::Mt) +
+                                sizeof(rng::MtRing);
+        BCK(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+        BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 256, smem_max));
+        per_sm = std::min(per_sm, 2);
+        if (per_sm < 1) throw std::runtime_error("batch kernel does not fit on an SM");
+    }
     const int budget = per_sm * nsm;
     if (n > budget) throw std::invalid_argument("more replicas than co-resident CTAs");
     // CTA groups: every replica gets its floor (below), then each further CTA
@@ -1064,7 +1074,7 @@ void BatchEngine::init() {
     BCK(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_launch));
     int fit = 0;
     BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, batch_kernel, 256, smem_launch));
-    if (fit < 1) throw std::runtime_error("batch kernel does not fit on an SM");
+    if (fit < per_sm) throw std::runtime_error("batch kernel does not fit its planned CTAs per SM");
     // per-replica device scratch
     std::vector<BatchRep> reps(n);
     std::vector<int2> map;

@@ -80,6 +80,18 @@ mgk_status mgk_ls_create(mgk_ls** out, int dim, int nx, int ny, int nz, int plan
     return MGK_OK;
 }
 
+mgk_status mgk_ls_set_precision(mgk_ls* h, int precision) {
+    if (!h || precision < 0 || precision > 1) return fail(MGK_BAD_ARG, "precision must be 0 (FP64) or 1 (FP32-refined)");
+    h->solver->set_precision(precision);
+    return MGK_OK;
+}
+
+mgk_status mgk_ls_last_solve_ms(mgk_ls* h, double* ms) {
+    if (!h || !ms) return fail(MGK_BAD_ARG, "null argument");
+    *ms = h->solver->last_solve_ms();
+    return MGK_OK;
+}
+
 mgk_status mgk_ls_solve(mgk_ls* h, const double* eps_bar, const double* eps_plastic, double* eps_inout, int warm,
                         double* sig_out, double* macro_out, int max_iter, double tol, int* iters_out) {
     if (!h || !eps_bar || !eps_inout) return fail(MGK_BAD_ARG, "null argument");

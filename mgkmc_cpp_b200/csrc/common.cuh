@@ -64,7 +64,9 @@ MGK_DEV unsigned long long global_ns() {
 }
 
 // A wait at a barrier gives up after this much device time.
-constexpr unsigned long long kBarrierTimeoutNs = 30ull * 1000000000ull;
+// (long enough for the longest one-CTA phase a group waits on: the catalog
+// and barrier redraw of a cascade of ~1e5 flips of 100 modes)
+constexpr unsigned long long kBarrierTimeoutNs = 120ull * 1000000000ull;
 
 // Sense-counting barrier for persistent kernels whose CTAs are co-resident
 // (launched cooperatively).  Every wait is bounded: after kBarrierTimeoutNs of

@@ -210,10 +210,16 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     smem_ = 2 * half_b;
     a.smem_half = (int)half_b;
     if (smem_ > 200 * 1024) throw std::invalid_argument("grid axis too long for the shared-memory FFT");
+    // the FP64 kernel and its FP32 twin (FP32-refined solves) share one grid:
+    // the smaller of their co-resident block counts
     auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
+    auto kfn32 = (D == 2) ? (const void*)ls_kernel<2, float> : (const void*)ls_kernel<3, float>;
     MGK_CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
-    int per_sm = 0;
+    MGK_CK(cudaFuncSetAttribute(kfn32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
+    int per_sm = 0, per_sm32 = 0;
     MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads_, smem_));
+    MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, kfn32, threads_, smem_));
+    per_sm = std::min(per_sm, per_sm32);
     if (per_sm < 1) throw std::runtime_error("LS kernel does not fit on an SM");
     grid_ = std::min(std::max(row_items, col_items), per_sm * nsm);
     grid_ = std::max(grid_, 1);
@@ -229,12 +235,16 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     alloc(&d_spec_, elem * S_ * (size_t)nrows * nh);
     alloc((void**)&d_partials_, sizeof(double) * kMaxPartials * grid_);
     alloc((void**)&d_res_, sizeof(LsResult));
+    alloc((void**)&d_res32_, sizeof(LsResult));
+    MGK_CK(cudaEventCreate(&ev0_));
+    MGK_CK(cudaEventCreate(&ev1_));
     alloc((void**)&d_bar_, sizeof(unsigned) * 4);
     MGK_CK(cudaMemcpy(d_lam_, lam.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
     MGK_CK(cudaMemcpy(d_mu_, mu.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
     MGK_CK(cudaMemset(d_eps_s_, 0, sizeof(double) * S_ * N));
     MGK_CK(cudaMemset(d_bar_, 0, sizeof(unsigned) * 4));
     MGK_CK(cudaMemset(d_res_, 0, sizeof(LsResult)));
+    MGK_CK(cudaMemset(d_res32_, 0, sizeof(LsResult)));
     a.eps_s = d_eps_s_;
     a.lam = d_lam_;
     a.mu = d_mu_;
@@ -252,6 +262,9 @@ LsSolver::~LsSolver() {
     cudaFree(d_spec_);
     cudaFree(d_partials_);
     cudaFree(d_res_);
+    cudaFree(d_res32_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
     cudaFree(d_bar_);
     for (void* p : tw_bufs_) cudaFree(p);
 }
@@ -288,11 +301,39 @@ cudaError_t LsSolver::solve(const double* ebar, bool warm, const double* epsp_s,
     a.max_iter = max_iter;
     a.tol = tol;
     a.epsp_s = epsp_s;
+    h_res32_ = LsResult{};
+    cudaEventRecord(ev0_, stream_);
+    if (precision_ == 1 && max_iter > 1) {
+        // FP32 phase: same passes on an FP32 spectrum (twiddles, Green
+        // operator and FFT arithmetic in FP32), its own result record
+        LsArgs a32 = a;
+        a32.tol = std::max(tol, kFp32Tol);
+        a32.max_iter = max_iter - 1;
+        a32.result = d_res32_;
+        void* p32[] = {&a32};
+        auto k32 = (D == 2) ? (const void*)ls_kernel<2, float> : (const void*)ls_kernel<3, float>;
+        cudaError_t e = cudaLaunchCooperativeKernel(k32, dim3(grid_), dim3(threads_), p32, smem_, stream_);
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpyAsync(&h_res32_, d_res32_, sizeof(LsResult), cudaMemcpyDeviceToHost, stream_);
+        if (e != cudaSuccess) return e;
+        // FP64 refinement from that field: a warm start whose mean is already
+        // eps_bar, every iteration FP64, to the requested tolerance
+        a.warm = 1;
+        a.norm_extra_first = a.norm_extra;
+        a.diff_extra_first = 0.0;
+        a.max_iter = max_iter;  // each phase has the caller's cap; the reported count is their sum
+    }
     void* params[] = {&a};
     auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
     cudaError_t e = cudaLaunchCooperativeKernel(kfn, dim3(grid_), dim3(threads_), params, smem_, stream_);
     if (e != cudaSuccess) return e;
+    cudaEventRecord(ev1_, stream_);
     return cudaMemcpyAsync(&h_res_, d_res_, sizeof(LsResult), cudaMemcpyDeviceToHost, stream_);
+}
+
+double LsSolver::last_solve_ms() const {
+    float ms = 0.f;
+    return cudaEventElapsedTime(&ms, ev0_, ev1_) == cudaSuccess ? (double)ms : -1.0;
 }
 
 void LsSolver::macro(double* em, double* sm, int* iters) const {
@@ -307,7 +348,7 @@ void LsSolver::macro(double* em, double* sm, int* iters) const {
             em[i * D + j] = h_res_.sum_s[c] * invN + sgn * w;
             sm[i * D + j] = h_res_.sum_sig[c] * invN + sgn * w * mean2mu;
         }
-    if (iters) *iters = h_res_.iters;
+    if (iters) *iters = h_res_.iters + h_res32_.iters;
 }
 
 unsigned LsSolver::device_error() const {

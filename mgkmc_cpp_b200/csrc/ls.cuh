@@ -25,6 +25,9 @@
 namespace mgk {
 
 constexpr int kMaxPartials = 16;
+// relative-change target of the FP32 phase of an FP32-refined solve: above
+// the FP32 rounding floor of the iteration (~1e-7 relative)
+constexpr double kFp32Tol = 1e-6;
 
 struct LsResult {
     int iters;
@@ -80,6 +83,15 @@ public:
     // current field and shift its mean to ebar (else fill with ebar).  epsp_s:
     // device S x N plastic strain or null.  Returns a cudaError_t.
     cudaError_t solve(const double* ebar, bool warm, const double* epsp_s, int max_iter, double tol);
+    // Precision of the iterations: 0 FP64 (the reference's), 1 FP32 spectrum
+    // and FFTs with an FP64 refinement: FP32 iterations (real-space fields,
+    // polarisation, norms and sums stay FP64) until the relative change is
+    // below max(tol, kFp32Tol), then FP64 iterations from that field to tol.
+    void set_precision(int p) { precision_ = p; }
+    int precision() const { return precision_; }
+    // device time of the last solve's launches (CUDA events on the solver's
+    // stream), after the stream has synchronised
+    double last_solve_ms() const;
 
     // After the stream has synchronised: mean strain / stress (full DxD
     // row-major) of the last solve and its iteration count.
@@ -119,6 +131,10 @@ private:
     void* d_spec_ = nullptr;
     LsResult* d_res_ = nullptr;
     LsResult h_res_{};
+    LsResult* d_res32_ = nullptr;  // result of the FP32 phase (precision 1)
+    LsResult h_res32_{};
+    int precision_ = 0;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     unsigned* d_bar_ = nullptr;  // {arrivals, generation, err}
     std::vector<void*> tw_bufs_;
     LsArgs args_{};

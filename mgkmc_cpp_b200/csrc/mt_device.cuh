@@ -173,7 +173,7 @@ namespace rng {
 // draw, only "where does the next accepted attempt start": the acceptance of
 // every attempt offset is computed in parallel, one thread walks the program
 // over those flags, and the values are computed in parallel per mode.
-constexpr int kRingGens = 4;
+constexpr int kRingGens = 8;
 constexpr int kRingWords = 624 * kRingGens;
 
 struct MtRing {
