@@ -348,7 +348,7 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the FP64 / FP32-refined LS block")
     ap.add_argument("--only-precision", action="store_true",
                     help="run only the FP64 / FP32-refined LS block and print its JSON (profiling the LS kernels)")
-    ap.add_argument("--ensemble-seconds", type=float, default=20.0)
+    ap.add_argument("--ensemble-seconds", type=float, default=40.0)
     ap.add_argument("--serve-jobs", type=int, default=40, help="jobs of the serving block (0: skip)")
     ap.add_argument("--serve-flips", type=int, nargs=2, default=[50, 500])
     ap.add_argument("--serve-full-sizes", action="store_true",

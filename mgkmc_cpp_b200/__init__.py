@@ -514,9 +514,10 @@ class Server:
             job["selected"].append(st["selected"])
             job["latency_us"].extend(st["event_us"].tolist())
             self.step_latency_us.extend(st["event_us"].tolist())
-            # a job without a decision (a sweep) for stall_seconds of device
-            # time is retired as stalled; cascade batches count as progress
-            job["idle_s"] = job["idle_s"] + ms / 1e3 if st["sweeps"] == 0 else 0.0
+            # a job without a thermal event for stall_seconds of device time
+            # (an avalanche whose cascade batches never settle -- the
+            # reference would run it forever) is retired as stalled
+            job["idle_s"] = job["idle_s"] + ms / 1e3 if st["events"] == 0 else 0.0
             job["stalled"] = job["idle_s"] >= self.stall_seconds
             if job["events"] >= job["target"] or st["terminated"] == 1 or job["stalled"]:
                 job["finished"] = now
