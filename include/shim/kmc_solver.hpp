@@ -8,8 +8,9 @@
 //
 // The simulation state lives on the device; the public field members
 // (eps_field, sig_field, eps_plastic, soft_prop) are host copies refreshed
-// after run_simulation and elastic_run.  Errors throw std::runtime_error;
-// fast patching (not built) throws at construction.
+// after run_simulation and elastic_run (with fast patching, sig_field is the
+// kept, stencil-updated stress, as in the reference).  Errors throw
+// std::runtime_error.
 #pragma once
 #include <Eigen/Dense>
 
