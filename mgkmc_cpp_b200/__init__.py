@@ -640,19 +640,22 @@ class KmcBatch:
         return float(ms[0])
 
     def stats(self, r: int) -> dict:
+        L = _lib.lib()
         out = np.zeros(19)
-        cap = 1 << 16
-        sel = (_lib.C.c_int * cap)()
         ln = _lib.C.c_longlong(0)
-        _lib.check(_lib.lib().mgk_batch_stats(self._h, r, _lib.dptr(out), sel, cap, _lib.C.byref(ln)))
+        _lib.check(L.mgk_batch_stats(self._h, r, _lib.dptr(out), None, 0, _lib.C.byref(ln)))  # counters, log length
         keys = ["events", "cascades", "cascade_flips", "ls_solves", "ls_iters", "elastic_steps", "fallbacks",
                 "min_margin", "terminated", "ctas", "ms_sweep", "ms_decide", "ms_event_solve", "ms_cascade_flips",
                 "ms_cascade_solve", "ms_interval_end", "sweeps", "h2d_bytes", "d2h_bytes"]
         d = {k: float(v) for k, v in zip(keys, out)}
-        d["selected"] = np.array(sel[:min(ln.value, cap)], dtype=np.int64)
-        us = np.zeros(cap)
-        _lib.check(_lib.lib().mgk_batch_event_times(self._h, r, _lib.dptr(us), cap, _lib.C.byref(ln)))
-        d["event_us"] = us[:min(ln.value, cap)].copy()
+        sel = np.zeros(max(ln.value, 1), dtype=np.int32)
+        _lib.check(L.mgk_batch_stats(self._h, r, _lib.dptr(out), sel.ctypes.data_as(_lib.C.POINTER(_lib.C.c_int)),
+                                     sel.size, _lib.C.byref(ln)))
+        d["selected"] = sel[:ln.value].astype(np.int64)
+        _lib.check(L.mgk_batch_event_times(self._h, r, None, 0, _lib.C.byref(ln)))
+        us = np.zeros(max(ln.value, 1))
+        _lib.check(L.mgk_batch_event_times(self._h, r, _lib.dptr(us), us.size, _lib.C.byref(ln)))
+        d["event_us"] = us[:ln.value].copy()
         return d
 
     def field(self, r: int, name: str) -> np.ndarray:
