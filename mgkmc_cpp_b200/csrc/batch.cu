@@ -163,7 +163,7 @@ MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
             const long i = m0 + (t << 5) + lane;
             r[k] = dd{0.0, 0.0};
             if (t < ntile && i < m1) {
-                const int v = (int)(i / R.s.M);
+                const int v = voxel_of(i, NM, R.s.M);
                 const double q = mode_Q<D, C>(R.s, R.p, v, i, time);
                 R.s.Q[i] = q;
                 bool inc;

@@ -46,6 +46,12 @@ MGK_DEV void voxel_stress(const KmcDevState& s, int v, double* sg) {
     for (int c = 0; c < S; ++c) sg[c] = m2 * e[c] + (c < D ? l * tr : 0.0);
 }
 
+// Voxel of flat mode index i (i < NM): a 32-bit division whenever the mode
+// count fits in 32 bits (the same quotient), the 64-bit one otherwise.
+MGK_DEV int voxel_of(long i, long NM, int M) {
+    return NM <= 0xffffffffL ? (int)((unsigned)i / (unsigned)M) : (int)(i / M);
+}
+
 // Q of mode i at voxel v (update_barriers, kmc_solver.hpp:345-407 / :1344-1406)
 template <int D, int C>
 MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, double time) {

@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(KmcDevState s, Kmc
     for (int j = 0; j < items; ++j) {
         const long i = base + (long)j * blockDim.x + threadIdx.x;
         if (i < s.NM) {
-            const int v = (int)(i / s.M);
+            const int v = voxel_of(i, s.NM, s.M);
             const double q = mode_Q<D, C>(s, p, v, i, time);
             s.Q[i] = q;
             bool inc;
