@@ -133,6 +133,18 @@ def traffic_from_profiles(workload: str):
     return float(m.group(1)) if m else None
 
 
+def batch_traffic_from_profiles(workload: str, events: float):
+    """DRAM bytes of a batch_kernel launch of `events` thermal events: the
+    committed ncu summary's bytes per event (a 4-replica, 20-event capture)
+    times the events, traffic growing with the events (each is a sweep and its
+    LS iterations).  None without the summary."""
+    p = os.path.join(HERE, "profiles", "batch_kernel_%sx4.md" % workload)
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_event:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) * events if m else None
+
+
 def run_reference(cfg_paths, n_events: int, timeout: float = 900.0):
     """Time the reference's own CPU path (oracle/_ref/ref_driver kmc_trace):
     the first n_events thermal events of every workload in cfg_paths, one
@@ -536,7 +548,9 @@ def main():
             "ls_voxel_iterations_per_s": iters * cfg.n_voxels / (ms / 1e3) if ms > 0 else None,
             "roofline": {"kernel": "batch_kernel (one persistent launch: every replica's sweeps, selections, flips, "
                                    "redraws and LS solves)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": batch_traffic_from_profiles(args.workload, ev),
+                         "traffic_note": "ncu DRAM bytes per event of a 20-event capture, times the launch's events",
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / max(ev2, 1),
                     "d2h_bytes_per_step": d2h / max(ev2, 1)},
