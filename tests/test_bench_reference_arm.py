@@ -23,3 +23,17 @@ def test_reference_arm_json_line():
         assert k in line, k
     assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] == 4
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_roofline_traffic_from_committed_profiles():
+    """The roofline's DRAM traffic comes from the committed ncu summaries: the
+    LS kernel's bytes per launch, and the batch kernel's bytes per event scaled
+    by the events of the timed launch."""
+    sys.path.insert(0, ROOT)
+    import bench
+    ls = bench.traffic_from_profiles("hetero2d_256")
+    assert ls is not None and ls > 0
+    per_event = bench.batch_traffic_from_profiles("hetero2d_256", 1)
+    assert per_event is not None and 1e6 < per_event < 1e9
+    assert bench.batch_traffic_from_profiles("hetero2d_256", 4000) == 4000 * per_event
+    assert bench.batch_traffic_from_profiles("no_such_workload", 4000) is None
