@@ -74,6 +74,17 @@ MGK_API mgk_status mgk_ls_set_precision(mgk_ls* h, int precision);
 /* Device time (ms, CUDA events on the solver's stream) of the last solve's
  * kernel launches, without its host copies. */
 MGK_API mgk_status mgk_ls_last_solve_ms(mgk_ls* h, double* ms);
+/* No counterpart in the reference (which has no device waits).  Every
+ * barrier wait inside the solver's persistent launch is bounded by device
+ * time; this sets the bound (seconds; 0 restores the 120 s default).  A wait
+ * that runs out makes every CTA of the launch return, and mgk_ls_solve then
+ * returns MGK_DEVICE_TIMEOUT with the handle still usable. */
+MGK_API mgk_status mgk_ls_set_wait_limit(mgk_ls* h, double seconds);
+/* Fault injection for failure-detection tests, no counterpart in the
+ * reference: cta >= 0 makes that CTA of the next solves leave before its first
+ * barrier (as if it had died), so the others' bounded waits run out; -1 turns
+ * it off.  The kernel never traps and never waits without a bound. */
+MGK_API mgk_status mgk_ls_inject_absent_cta(mgk_ls* h, int cta);
 MGK_API void mgk_ls_destroy(mgk_ls* h);
 
 /* ---------------------------------------------------------------- LS solve without allocating
@@ -89,11 +100,14 @@ MGK_API void mgk_ls_destroy(mgk_ls* h);
  * default stream).  The call returns after the stream has finished the solve.
  * Nothing is allocated: every intermediate lives in one static device array of
  * MGK_NOALLOC_SCRATCH_BYTES (16 MiB), which every GPU that loads the library
- * holds until the process exits; grids whose intermediates exceed it (about
- * 88 bytes per voxel in 2D, 170 in 3D; e.g. up to 256x256 in 2D or 40^3 in
- * 3D) are refused with MGK_BAD_SHAPE.  The first call on a device looks up the
- * array's device address (and may load the library's GPU code), so make that
- * first call before any stream capture.  All calls share the one array, which
+ * holds until the process exits; grids whose intermediates exceed it are
+ * refused with MGK_BAD_SHAPE.  The intermediates take about 88 bytes per voxel
+ * in 2D and 170 in 3D with a plastic strain (64 and 112 without), so the limit
+ * is about 190k voxels in 2D and 98k in 3D: 432x432 fits and 448x432 does not
+ * (2D with a plastic strain); 44^3 fits and 48^3 does not (3D).  Every call
+ * looks up the array's device address on the current device (the first one
+ * may load the library's GPU code), so make the first call before any stream
+ * capture.  All calls share the one array, which
  * keeps the previous call's contents (each call resets what must start at
  * zero): calls that overlap on the GPU, from several streams or threads, race
  * and must be serialised by the caller.  mgk_noalloc_last_error() describes

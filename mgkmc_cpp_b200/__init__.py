@@ -78,6 +78,15 @@ class LsSolver:
             raise ValueError("precision must be 'fp64' or 'fp32_refined'")
         _lib.check(L.mgk_ls_set_precision(h, 1 if precision == "fp32_refined" else 0))
 
+    def set_wait_limit(self, seconds: float):
+        """Bound of every device-side barrier wait of the solver (0: 120 s)."""
+        _lib.check(_lib.lib().mgk_ls_set_wait_limit(self._h, float(seconds)))
+
+    def inject_absent_cta(self, cta: int):
+        """Failure-detection tests: CTA ``cta`` of the next solves leaves before
+        its first barrier (-1: off)."""
+        _lib.check(_lib.lib().mgk_ls_inject_absent_cta(self._h, int(cta)))
+
     def last_solve_ms(self) -> float:
         """Device time of the last solve's kernels (no host copies)."""
         ms = np.zeros(1)

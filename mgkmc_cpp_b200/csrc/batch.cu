@@ -747,7 +747,7 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
     rng::MtRing& s_ring = *reinterpret_cast<rng::MtRing*>(smem + smem_bytes + sizeof(rng::Mt));
     __shared__ int s_flag;
     BatchCtl* c = R.ctl;
-    const GridBar gb{R.bar, (unsigned)R.ncta, R.bar + 2};
+    const GridBar gb{R.bar, (unsigned)R.ncta, R.bar + 2, kBarrierTimeoutNs};
     if (rank == 0) {
         for (int i = threadIdx.x; i < 624; i += blockDim.x) s_mt.mt[i] = R.mt->mt[i];
         if (threadIdx.x == 0) s_mt.idx = R.mt->idx;
@@ -1007,7 +1007,7 @@ void BatchEngine::init() {
     {
         const size_t smem_max = std::max({(size_t)4096 * 12, kRedrawSmem, 2 * half_budget}) + sizeof(rng::Mt) +
                                 sizeof(rng::MtRing);
-        BCK(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+        BCK(ensure_dyn_smem((const void*)batch_kernel, smem_max));
         BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 256, smem_max));
         per_sm = std::min(per_sm, 2);
         if (per_sm < 1) throw std::runtime_error("batch kernel does not fit on an SM");
@@ -1076,7 +1076,7 @@ void BatchEngine::init() {
     }
     smem_ = (smem_ + 15) & ~(size_t)15;
     const size_t smem_launch = smem_ + sizeof(rng::Mt) + sizeof(rng::MtRing);
-    BCK(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_launch));
+    BCK(ensure_dyn_smem((const void*)batch_kernel, smem_launch));
     int fit = 0;
     BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, batch_kernel, 256, smem_launch));
     if (fit < per_sm) throw std::runtime_error("batch kernel does not fit its planned CTAs per SM");

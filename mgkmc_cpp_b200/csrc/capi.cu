@@ -86,6 +86,19 @@ mgk_status mgk_ls_set_precision(mgk_ls* h, int precision) {
     return MGK_OK;
 }
 
+mgk_status mgk_ls_set_wait_limit(mgk_ls* h, double seconds) {
+    if (!h || !(seconds >= 0.0) || seconds > 1e6) return fail(MGK_BAD_ARG, "wait limit must be in [0, 1e6] seconds");
+    h->solver->set_wait_limit_ns((unsigned long long)(seconds * 1e9));
+    return MGK_OK;
+}
+
+mgk_status mgk_ls_inject_absent_cta(mgk_ls* h, int cta) {
+    if (!h || cta < -1) return fail(MGK_BAD_ARG, "cta must be -1 (off) or a CTA index");
+    if (cta >= h->solver->grid()) return fail(MGK_BAD_ARG, "cta beyond the solver's grid");
+    h->solver->set_test_absent_cta(cta);
+    return MGK_OK;
+}
+
 mgk_status mgk_ls_last_solve_ms(mgk_ls* h, double* ms) {
     if (!h || !ms) return fail(MGK_BAD_ARG, "null argument");
     *ms = h->solver->last_solve_ms();

@@ -3,7 +3,24 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #define MGK_DEV __device__ __forceinline__
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` and never
+// lowers it.  The attribute belongs to the function (per device), not to the
+// object that plans a launch: two solvers of different sizes share it, so
+// setting it to one launch's own need would make the other's larger launch
+// fail with cudaErrorInvalidValue.
+inline cudaError_t ensure_dyn_smem(const void* fn, size_t bytes) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+    if (e != cudaSuccess) return e;
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 
 // ---------------------------------------------------------------- error words
 // Device kernels never trap: a failed bounded wait or a bad size sets a bit in
@@ -63,20 +80,21 @@ MGK_DEV unsigned long long global_ns() {
     return t;
 }
 
-// A wait at a barrier gives up after this much device time.
+// Default limit of one wait at a barrier, in device time.
 // (long enough for the longest one-CTA phase a group waits on: the catalog
 // and barrier redraw of a cascade of ~1e5 flips of 100 modes)
 constexpr unsigned long long kBarrierTimeoutNs = 120ull * 1000000000ull;
 
 // Sense-counting barrier for persistent kernels whose CTAs are co-resident
-// (launched cooperatively).  Every wait is bounded: after kBarrierTimeoutNs of
-// device time (or as soon as another CTA has given up) the CTA records
+// (launched cooperatively).  Every wait is bounded: after limit_ns of device
+// time (or as soon as another CTA has given up) the CTA records
 // MGK_DERR_BARRIER_TIMEOUT and the barrier reports failure, so a kernel never
 // spins forever.  `bar` points at two words: {arrivals, generation}.
 struct GridBar {
     unsigned* bar;
     unsigned nblocks;
     unsigned* err;
+    unsigned long long limit_ns;
 };
 
 MGK_DEV bool grid_sync(const GridBar& g) {
@@ -98,7 +116,7 @@ MGK_DEV bool grid_sync(const GridBar& g) {
             while (*gen == my_gen) {
                 __nanosleep(32);
                 if ((*(volatile unsigned*)g.err & MGK_DERR_BARRIER_TIMEOUT) ||
-                    ((++polls & 255u) == 0 && global_ns() - t0 > kBarrierTimeoutNs)) {
+                    ((++polls & 255u) == 0 && global_ns() - t0 > g.limit_ns)) {
                     atomicOr(g.err, MGK_DERR_BARRIER_TIMEOUT);
                     ok = 0;
                     break;

@@ -79,18 +79,6 @@ double BarrierGen::generate(std::mt19937& rng) const {
 
 static const double kB = 8.617e-5;
 
-// Opt-in host-side trace of the run loop (environment MGK_DEBUG=<max lines>).
-static long g_debug_left = -1;
-static bool dbg() {
-    if (g_debug_left < 0) {
-        const char* e = std::getenv("MGK_DEBUG");
-        g_debug_left = e ? std::atol(e) : 0;
-    }
-    if (g_debug_left <= 0) return false;
-    --g_debug_left;
-    return true;
-}
-
 KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu) : p_(p), rng_((unsigned)p.seed) {
     if (p.dim != 2 && p.dim != 3) throw std::invalid_argument("dim must be 2 or 3");
     if (p.nx < 1 || p.ny < 1 || (p.dim == 3 && p.nz < 1) || p.M < 1) throw std::invalid_argument("bad grid or M");
@@ -528,7 +516,6 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips, long long cap) {
         CK(cudaStreamSynchronize(st_));
         stats_.syncs++;
         const int n = h_status_->n_collect;
-        if (dbg()) fprintf(stderr, "[mgk] cascade collect: n_unstable %d collected %d\n", h_status_->n_unstable, n);
         if (n <= 0) break;
         // draws of the n flips in flip order (one normal object per flip)
         const size_t need = (size_t)n * rec;
@@ -558,7 +545,6 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips, long long cap) {
         } else {
             CK(enqueue_elastic());
         }
-        if (dbg()) fprintf(stderr, "[mgk] cascade batch %d flips %d\n", local, n);
         total += n;
         ++local;
         CK(enqueue_sweep());
@@ -715,7 +701,6 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
     };
     int elastic_done = 0, total_kmc = 0, step = 1, seq_instab = 0;
     const long long events_at_start = stats_.thermal_events;
-    g_debug_left = -1;  // re-read MGK_DEBUG for this run
     const int max_seq = (int)(rp.max_kmc_steps_pct * (double)N_);
     mgk_status s;
     try {
@@ -723,7 +708,6 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
         CK(enqueue_elastic());
         CK(enqueue_sweep());
         s = sync_status();
-        if (dbg()) fprintf(stderr, "[mgk] run start: LS iters %d, n_unstable %d, status %d\n", h_lsres_->iters, h_status_->n_unstable, (int)s);
         if (s != MGK_OK) return s;
         if (console_) {
             fputs("Timestamp              Elapsed(s)   Step     Type            Eps_xx       Sig_xx(GPa)     KMC      Cascade  Flips    SimTime(s)\n", stdout);
@@ -756,9 +740,6 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                 }
                 const double R = h_status_->total_hi + h_status_->total_lo;
                 const double t_ev = wall_seconds();
-                if (dbg())
-                    fprintf(stderr, "[mgk] loop R=%.6e remaining=%.6e n_unstable=%d events=%lld time=%.9e\n", R, remaining,
-                            h_status_->n_unstable, stats_.thermal_events, time_);
                 if (R > 0.0) {
                     const double u1 = U(rng_);
                     const double tw = -std::log(u1) / R;
@@ -832,10 +813,8 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
             for (double v : nu_) ns += v;
             const double Ea = Es / E_.size(), na = ns / nu_.size();
             int solves = 0;
-            if (dbg()) fprintf(stderr, "[mgk] mixed-BC loop, elastic step %d\n", elastic_done + 1);
             for (int it = 0; it < rp.mixed_max_iter; ++it) {
                 s = elastic_run();
-                if (dbg()) fprintf(stderr, "[mgk]   mixed it %d iters %d sig_macro %.6e %.6e\n", it, h_lsres_->iters, sig_macro_[0], sig_macro_[D * D - 1]);
                 if (s != MGK_OK) {
                     close_logs();
                     return s;

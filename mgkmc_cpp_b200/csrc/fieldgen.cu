@@ -245,7 +245,7 @@ void correlated_field(int dim, int nx, int ny, int nz, double mean, double sd, d
                 const size_t line_b = (size_t)(n + (n >> 3) + 1) * sizeof(cplx<double>);
                 int per = (int)std::max<size_t>(1, std::min<size_t>(64, (48 * 1024) / (2 * line_b)));
                 const size_t smem = 2 * per * line_b;
-                if (smem > 48 * 1024) FCK(cudaFuncSetAttribute(fft_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                if (smem > 48 * 1024) FCK(ensure_dyn_smem((const void*)fft_axis_kernel, smem));
                 const long nlines = N / n;
                 const int grid = (int)std::min<long>((nlines + per - 1) / per, 1184);
                 fft_axis_kernel<<<grid, 256, smem, st>>>(z, nx, ny, nz, a, ax[a], per, sign);

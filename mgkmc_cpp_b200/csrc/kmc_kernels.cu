@@ -483,7 +483,7 @@ cudaError_t kmc_cascade_flip(const KmcDevState& s, const KmcPhys& p, double* key
     if (npow2 <= 8192) {
         const size_t smem = (size_t)npow2 * (sizeof(double) + sizeof(int));
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(bitonic_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaError_t e = ensure_dyn_smem((const void*)bitonic_smem_kernel, smem);
             if (e != cudaSuccess) return e;
         }
         bitonic_smem_kernel<<<1, 1024, smem, st>>>(keys, modes, n, npow2);

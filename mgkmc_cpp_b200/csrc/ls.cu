@@ -40,7 +40,7 @@ using namespace lsdev;
 template <int D, typename T>
 __global__ void __launch_bounds__(256, 2) ls_kernel(const __grid_constant__ LsArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const GridBar gb{a.bar, gridDim.x, a.err};
+    const GridBar gb{a.bar, gridDim.x, a.err, a.wait_ns ? a.wait_ns : kBarrierTimeoutNs};
     ls_solve_group<D, T>(a, blockIdx.x, gridDim.x, gb, smem_raw);
 }
 
@@ -214,8 +214,8 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     // the smaller of their co-resident block counts
     auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
     auto kfn32 = (D == 2) ? (const void*)ls_kernel<2, float> : (const void*)ls_kernel<3, float>;
-    MGK_CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
-    MGK_CK(cudaFuncSetAttribute(kfn32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_));
+    MGK_CK(ensure_dyn_smem(kfn, smem_));
+    MGK_CK(ensure_dyn_smem(kfn32, smem_));
     int per_sm = 0, per_sm32 = 0;
     MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads_, smem_));
     MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, kfn32, threads_, smem_));
@@ -357,7 +357,12 @@ unsigned LsSolver::device_error() const {
     return e;
 }
 
-void LsSolver::clear_error() { cudaMemset(d_bar_, 0, sizeof(unsigned) * 4); }
+// on the solver's own (non-blocking) stream, so that the next launch on it
+// sees the cleared words
+void LsSolver::clear_error() {
+    cudaMemsetAsync(d_bar_, 0, sizeof(unsigned) * 4, stream_);
+    cudaStreamSynchronize(stream_);
+}
 
 cudaError_t LsSolver::download_eps(double* host) const {
     double* tmp = nullptr;
@@ -437,26 +442,17 @@ namespace {
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[MGK_NOALLOC_SCRATCH_BYTES];
 
-std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_ptr[64] = {nullptr};
-
 // Device address of the scratch array on the current device.  In host code the
 // symbol g_noalloc_scratch only names a host-side stand-in, so it is never
-// passed to a kernel; the address comes from cudaGetSymbolAddress, looked up
-// once per device with that device current.
+// passed to a kernel; the address comes from cudaGetSymbolAddress with the
+// device current.  It is looked up on every call (cheap once the module is
+// loaded) rather than cached, so that a context re-created after
+// cudaDeviceReset gets its own, valid address.
 cudaError_t noalloc_scratch(unsigned char** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = g_noalloc_ptr[dev];
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 
@@ -572,7 +568,7 @@ mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stres
     a.smem_half = (int)half_b;
     if (smem > 200 * 1024) return noalloc_fail(MGK_BAD_SHAPE, "grid axis too long for the shared-memory FFT");
     auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
-    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (ensure_dyn_smem(kfn, smem) != cudaSuccess)
         return noalloc_fail(MGK_CUDA_ERROR, "cannot configure the LS kernel");
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, 256, smem) != cudaSuccess || per_sm < 1)

@@ -64,6 +64,9 @@ struct LsArgs {
     LsResult* result;
     unsigned* bar;
     unsigned* err;
+    unsigned long long wait_ns;  // limit of one barrier wait (0: kBarrierTimeoutNs)
+    int test_absent;       // fault injection: k > 0 makes CTA k-1 leave before its first barrier
+    int pad1;
     FftAxis ax[3];         // per axis (x, y, z)
 };
 
@@ -88,6 +91,13 @@ public:
     // polarisation, norms and sums stay FP64) until the relative change is
     // below max(tol, kFp32Tol), then FP64 iterations from that field to tol.
     void set_precision(int p) { precision_ = p; }
+    // Limit of every device-side barrier wait of this solver's launches
+    // (0: the 120 s default); a wait that runs out ends the launch with the
+    // error word set (MGK_DEVICE_TIMEOUT on the C ABI).
+    void set_wait_limit_ns(unsigned long long ns) { args_.wait_ns = ns; }
+    // Fault injection for tests: cta >= 0 makes that CTA of the next solves
+    // leave before its first barrier; -1 turns it off.
+    void set_test_absent_cta(int cta) { args_.test_absent = cta >= 0 ? cta + 1 : 0; }
     int precision() const { return precision_; }
     // device time of the last solve's launches (CUDA events on the solver's
     // stream), after the stream has synchronised

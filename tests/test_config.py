@@ -6,7 +6,8 @@ import pytest
 
 from mgkmc_cpp_b200.config import SimConfig, YAMLConfig, _stod, _stoi
 
-REF = "/root/reference"
+# the reference source tree, when the environment names one (its example configs)
+REF = os.environ.get("MGK_REFERENCE_DIR", "")
 
 
 def test_yaml_flat_keys_comments_quotes():
@@ -101,7 +102,7 @@ material:
 """))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not mounted")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="MGK_REFERENCE_DIR not set to the reference tree")
 def test_reference_example_configs_parse():
     n = 0
     for root, _, files in os.walk(os.path.join(REF, "examples")):

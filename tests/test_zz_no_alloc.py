@@ -103,13 +103,45 @@ def test_noalloc_matches_allocating_solver_twice_in_a_row(env):
     assert again[3] == ref[3] and rel(again[0], ref[0]) < 1e-12 and rel(again[1], ref[1]) < 1e-12
 
 
+def _noalloc_status(env, dims, plastic):
+    torch, G, L = env
+    D, N = len(dims), int(np.prod(dims))
+    t = torch.full((N,), 90e9, dtype=torch.float64, device="cuda")
+    nu = torch.full((N,), 0.3, dtype=torch.float64, device="cuda")
+    e = torch.zeros((N, D * D), dtype=torch.float64, device="cuda")
+    ep = torch.zeros((N, D * D), dtype=torch.float64, device="cuda") if plastic else None
+    eb = np.zeros(D * D)
+    eb[0] = 1e-3
+    it = C.c_int(0)
+    st = L.mgk_ls_solve_noalloc(D, dims[0], dims[1], dims[2] if D == 3 else 1, 0, 1.0, t.data_ptr(), nu.data_ptr(),
+                                G._lib.dptr(eb), ep.data_ptr() if ep is not None else None, e.data_ptr(), 0, None, None,
+                                5, 1e-6, C.byref(it), None)
+    torch.cuda.synchronize()
+    return st
+
+
 def test_noalloc_refuses_grids_beyond_its_static_scratch(env):
     torch, G, L = env
-    N = 512 * 512
-    t = torch.full((N,), 90e9, dtype=torch.float64, device="cuda")
-    e = torch.zeros((N, 4), dtype=torch.float64, device="cuda")
-    eb = np.zeros(4)
-    st = L.mgk_ls_solve_noalloc(2, 512, 512, 1, 0, 1.0, t.data_ptr(), t.data_ptr(), G._lib.dptr(eb), None, e.data_ptr(), 0,
-                                None, None, 10, 1e-6, None, None)
-    assert st == 2  # MGK_BAD_SHAPE
-    assert b"static limit" in L.mgk_noalloc_last_error()
+    # 16 MiB of scratch: just below the limit, 2D with a plastic strain and 3D
+    assert _noalloc_status(env, (432, 432), True) in (0, 1)
+    assert _noalloc_status(env, (44, 44, 44), True) in (0, 1)
+    # just above it, and far above it
+    for dims, plastic in (((448, 432), True), ((48, 48, 48), True), ((512, 512), False)):
+        assert _noalloc_status(env, dims, plastic) == 2  # MGK_BAD_SHAPE
+        assert b"static limit" in L.mgk_noalloc_last_error()
+
+
+def test_noalloc_leaves_other_solvers_launchable(env):
+    # the kernel's dynamic shared-memory limit is process-wide: a no-alloc
+    # call on a small grid must not lower it below what a live solver of a
+    # larger grid planned for
+    torch, G, L = env
+    big = (384, 512)  # row pass of 512-point lines: above the 48 KiB default limit
+    E, nu, eb, epsp, eps0 = case(big, 21, False, False)
+    s = G.LsSolver(big, E, nu, "plane_strain", 1.0)
+    ref = s.solve(eb, None, None, 200, 1e-8)
+    small = (12, 10)
+    solve_noalloc(env, small, *case(small, 22, False, False), False, 50, 1e-8)
+    again = s.solve(eb, None, None, 200, 1e-8)
+    s.close()
+    assert again[4] == ref[4] and rel(again[0], ref[0]) < 1e-12
