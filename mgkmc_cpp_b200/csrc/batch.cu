@@ -923,31 +923,6 @@ __global__ void __launch_bounds__(256, 2) batch_kernel(BatchRep* reps, const int
         if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
     } while (0)
 
-// Re-plans the LS pass tiling of one replica for its group of ncta CTAs: row
-// chunks of rpb rows and column tiles of tk half-spectrum columns as large as
-// half_budget bytes of shared memory allow while every CTA still gets work,
-// so that a small group runs few, wide FFT batches instead of many narrow
-// ones.  Returns the bytes of one of the two FFT buffers.
-static size_t replan_ls(LsArgs& a, int D, int ncta, size_t half_budget) {
-    const int S = D == 2 ? 3 : 6;
-    const size_t elem = sizeof(cplx<double>);
-    auto padded = [](int n) { return (size_t)n + (size_t)(n >> 3) + 1; };
-    auto row_b = [&](int rpb) { return (size_t)((rpb * S + 1) / 2) * padded(a.nr) * elem; };
-    int rpb_max = 1;
-    while (rpb_max < a.nrows && row_b(rpb_max + 1) <= half_budget) ++rpb_max;
-    const int per_cta = (a.nrows + ncta * rpb_max - 1) / (ncta * rpb_max);
-    a.rpb = std::max(1, std::min(rpb_max, (a.nrows + ncta * per_cta - 1) / (ncta * per_cta)));
-    size_t colp = 0;
-    for (int ax = 0; ax < D - 1; ++ax) colp = std::max(colp, padded(a.dims[ax]));
-    int tk_max = 1;
-    while (tk_max < a.nh && (size_t)S * (tk_max + 1) * colp * elem <= half_budget) ++tk_max;
-    const int no_min = D == 2 ? 1 : std::min(a.dims[0], a.dims[1]);
-    const int tiles = std::max(1, (ncta + no_min - 1) / no_min);  // column tiles wanted per outer index
-    a.tk = std::max(1, std::min(tk_max, (a.nh + tiles - 1) / tiles));
-    const size_t half = std::max(row_b(a.rpb), (size_t)S * a.tk * colp * elem);
-    return (half + 127) / 128 * 128;
-}
-
 BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* const* E, const double* const* nu) {
     if (n < 1) throw std::invalid_argument("empty batch");
     // replicas are built concurrently: each one's initial catalog and barrier
@@ -1001,11 +976,13 @@ void BatchEngine::init() {
     // CTA per SM, measured on B200); the dynamic shared memory of each holds
     // two LS FFT buffers (or the cascade sort / redraw scratch) and, past
     // them, the replica generator
-    const size_t half_budget = 36 * 1024;
+    // shared memory of a replica's LS passes (line buffer + twiddle table);
+    // the group tiling (plan_passes) fills it
+    const size_t ls_budget = 72 * 1024;
     // CTAs per SM: two when the largest launch this plan can make fits twice
     int per_sm = 0;
     {
-        const size_t smem_max = std::max({(size_t)4096 * 12, kRedrawSmem, 2 * half_budget}) + sizeof(rng::Mt) +
+        const size_t smem_max = std::max({(size_t)4096 * 12, kRedrawSmem, ls_budget}) + sizeof(rng::Mt) +
                                 sizeof(rng::MtRing);
         BCK(ensure_dyn_smem((const void*)batch_kernel, smem_max));
         BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 256, smem_max));
@@ -1069,10 +1046,12 @@ void BatchEngine::init() {
     std::vector<LsArgs> plans(n);
     smem_ = std::max((size_t)4096 * 12, kRedrawSmem);
     for (int r = 0; r < n; ++r) {
+        // the LS pass tiling re-planned for the replica's group: chunks and
+        // tiles as large as the budget allows while every CTA has work
         plans[r] = eng_[r]->ls_->args_;
-        const size_t half = replan_ls(plans[r], eng_[r]->D_, ncta_[r], half_budget);
-        plans[r].smem_half = (int)half;
-        smem_ = std::max(smem_, 2 * half);
+        const size_t need = plan_passes(plans[r], ncta_[r], ls_budget);
+        if (need == 0) throw std::invalid_argument("grid axis too long for the batched LS passes");
+        smem_ = std::max(smem_, need);
     }
     smem_ = (smem_ + 15) & ~(size_t)15;
     const size_t smem_launch = smem_ + sizeof(rng::Mt) + sizeof(rng::MtRing);
@@ -1115,7 +1094,8 @@ void BatchEngine::init() {
         alloc((void**)&R.ctl, sizeof(BatchCtl));
         alloc((void**)&R.sel_log, sizeof(int) * kSelLog);
         alloc((void**)&R.ev_ns, sizeof(unsigned long long) * kSelLog);
-        alloc((void**)&R.ls.partials, sizeof(double) * kMaxPartials * R.ncta);
+        alloc((void**)&R.ls.partials, sizeof(double) * kMaxPartials * (R.ncta + 1));
+        R.ls.red = R.ls.partials + (size_t)kMaxPartials * R.ncta;
         alloc((void**)&R.ls.result, sizeof(LsResult));
         R.ls.bar = R.bar;
         R.ls.err = R.bar + 2;

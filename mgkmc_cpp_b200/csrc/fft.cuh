@@ -20,10 +20,26 @@ constexpr int kMaxStages = 24;
 struct FftAxis {
     int n;
     int nst;
+    int lw;  // lines a warp transforms together (warp-owned path, n <= kWarpFftMax)
+    int pad;
     int radix[kMaxStages];
     const cplx<double>* tw64;  // length n
     const cplx<float>* tw32;   // length n
 };
+
+// Longest line the warp-owned transforms take; longer lines use the CTA-wide
+// path (fft_lines).
+constexpr int kWarpFftMax = 512;
+
+// Lines of length n a warp transforms together: enough that every stage has
+// at least 32 butterflies when n is small (1 for n >= 256); 0 when n is too
+// long for the warp-owned path.
+__host__ __device__ inline int warp_lines(const FftAxis& a) {
+    if (a.n > kWarpFftMax) return 0;
+    int lw = 1;
+    while (lw * a.n < 256) lw *= 2;
+    return lw;
+}
 
 template <typename T>
 MGK_DEV const cplx<T>* tw_of(const FftAxis& a);
@@ -132,7 +148,7 @@ MGK_DEV void fft_stage(const cplx<T>* __restrict__ in, cplx<T>* __restrict__ out
 // Runs all stages of `ax` over `nlines` lines held in `a`; `b` is scratch of the
 // same size.  Returns the buffer that holds the result.  Contains __syncthreads.
 template <typename T>
-MGK_DEV cplx<T>* fft_lines(cplx<T>* a, cplx<T>* b, int nlines, const FftAxis& ax, int sign) {
+__device__ __noinline__ cplx<T>* fft_lines(cplx<T>* a, cplx<T>* b, int nlines, const FftAxis& ax, int sign) {
     const cplx<T>* tw = tw_of<T>(ax);
     int Ns = 1;
     for (int s = 0; s < ax.nst; ++s) {
@@ -153,6 +169,99 @@ MGK_DEV cplx<T>* fft_lines(cplx<T>* a, cplx<T>* b, int nlines, const FftAxis& ax
         __syncthreads();
     }
     return a;
+}
+
+// ---------------------------------------------------------------- warp-owned transforms
+// One Stockham stage (the arithmetic of fft_stage) of `cnt` lines of length
+// n owned by one warp: lane after lane takes a butterfly, reads its R inputs
+// from `in`, writes its R outputs to their autosorted positions in `out`, and
+// the warp synchronises at the end.  tw is a shared-memory copy of the axis
+// table.
+template <typename T, int R>
+MGK_DEV void warp_stage(const cplx<T>* __restrict__ in, cplx<T>* __restrict__ out, int lsn, int cnt, int n, int Ns,
+                        const cplx<T>* __restrict__ tw, int sign) {
+    const int m = n / R;
+    const int nb = cnt * m;
+    const int tstep = n / (Ns * R);
+    for (int b = threadIdx.x & 31; b < nb; b += 32) {
+        const int l = b / m, j = b - l * m;
+        const cplx<T>* src = in + l * lsn;
+        cplx<T>* dst = out + l * lsn;
+        const int k = j % Ns;
+        cplx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[pad_idx(j + r * m)];
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                cplx<T> w = tw[r * k * tstep];
+                if (sign > 0) w = cconj(w);
+                v[r] = cmul(v[r], w);
+            }
+        }
+        small_dft<T, R>(v, sign, tw, n);
+        const int d = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[pad_idx(d + r * Ns)] = v[r];
+    }
+    __syncwarp();
+}
+
+// All stages of `nlines` lines (stride lsn) held in a, with b as the second
+// buffer: each group of ax.lw lines is transformed by one warp, the warps of
+// the CTA taking the groups in turn, so the stages need no CTA barrier.
+// Returns the buffer holding the result (a after an even number of stages,
+// else b, for every line).  The caller synchronises the CTA before other
+// warps read the lines.  One out-of-line copy per type keeps the persistent
+// kernels' code small.
+template <typename T>
+__device__ __noinline__ cplx<T>* fft_lines_warp(cplx<T>* a, cplx<T>* b, int nlines, int lsn, const FftAxis& ax,
+                                                const cplx<T>* tw, int sign) {
+    const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lw = ax.lw;
+    const int ngroups = (nlines + lw - 1) / lw;
+    for (int g = wid; g < ngroups; g += nw) {
+        const int l0 = g * lw;
+        const int cnt = min(lw, nlines - l0);
+        cplx<T>* x = a + l0 * lsn;
+        cplx<T>* y = b + l0 * lsn;
+        int Ns = 1;
+        for (int s = 0; s < ax.nst; ++s) {
+            const int R = ax.radix[s];
+            switch (R) {
+                case 2: warp_stage<T, 2>(x, y, lsn, cnt, ax.n, Ns, tw, sign); break;
+                case 3: warp_stage<T, 3>(x, y, lsn, cnt, ax.n, Ns, tw, sign); break;
+                case 4: warp_stage<T, 4>(x, y, lsn, cnt, ax.n, Ns, tw, sign); break;
+                case 5: warp_stage<T, 5>(x, y, lsn, cnt, ax.n, Ns, tw, sign); break;
+                case 7: warp_stage<T, 7>(x, y, lsn, cnt, ax.n, Ns, tw, sign); break;
+                case 8: warp_stage<T, 8>(x, y, lsn, cnt, ax.n, Ns, tw, sign); break;
+                default: break;
+            }
+            Ns *= R;
+            cplx<T>* t = x;
+            x = y;
+            y = t;
+        }
+    }
+    return (ax.nst & 1) ? b : a;
+}
+
+// Copies the axis twiddle table to shared memory (warp-owned path); the
+// caller synchronises before use.
+template <typename T>
+MGK_DEV void load_twiddles(const FftAxis& ax, cplx<T>* tw_s) {
+    if (ax.lw == 0) return;
+    const cplx<T>* tw = tw_of<T>(ax);
+    for (int i = threadIdx.x; i < ax.n; i += blockDim.x) tw_s[i] = tw[i];
+}
+
+// Transform of `nlines` lines starting at a, with b as the second buffer:
+// warp-owned when the axis allows it, else CTA-wide.  Returns the buffer
+// holding the result.  The caller synchronises the CTA after it.
+template <typename T>
+MGK_DEV cplx<T>* fft_any(cplx<T>* a, cplx<T>* b, int nlines, const FftAxis& ax, const cplx<T>* tw_s, int sign) {
+    if (ax.lw > 0) return fft_lines_warp<T>(a, b, nlines, pad_len(ax.n), ax, tw_s, sign);
+    return fft_lines<T>(a, b, nlines, ax, sign);
 }
 
 }  // namespace mgk

@@ -103,7 +103,7 @@ __global__ void split_tensor_kernel(const double* __restrict__ full, int N, doub
 // shared-memory line length of a length-n transform (pad_len in fft.cuh)
 static size_t padded_len(int n) { return (size_t)n + (size_t)(n >> 3) + 1; }
 
-bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned) {
+bool plan_radices(int n, FftAxis* ax) {
     std::memset(ax, 0, sizeof(*ax));
     ax->n = n;
     int m = n, k = 0;
@@ -114,6 +114,12 @@ bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned) {
         while (m % p == 0 && k < kMaxStages) { ax->radix[k++] = p; m /= p; }
     if (m != 1) return false;
     ax->nst = k;
+    ax->lw = warp_lines(*ax);
+    return true;
+}
+
+bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned) {
+    if (!plan_radices(n, ax)) return false;
     std::vector<double> t64(2 * (size_t)n);
     std::vector<float> t32(2 * (size_t)n);
     for (int i = 0; i < n; ++i) {
@@ -133,6 +139,54 @@ bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned) {
     ax->tw64 = reinterpret_cast<const cplx<double>*>(d64);
     ax->tw32 = reinterpret_cast<const cplx<float>*>(d32);
     return true;
+}
+
+int plan_items(const LsArgs& a) {
+    const int row_items = (a.nrows + a.rpb - 1) / a.rpb;
+    const int no = a.D == 2 ? 1 : std::min(a.dims[0], a.dims[1]);
+    const int col_items = no * ((a.nh + a.tk - 1) / a.tk);
+    return std::max(row_items, col_items);
+}
+
+size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, int rpb, int tk) {
+    const int D = a.D, S = a.S;
+    ncta = std::max(ncta, 1);
+    a.nhs = (a.nh + 3) / 4 * 4;
+    const size_t elem = sizeof(cplx<double>);  // the FP32 kernel uses half of it
+    auto al = [](size_t b) { return (b + 127) / 128 * 128; };
+    const bool two = true;  // both transform paths run between two line buffers
+    size_t maxn = a.nr;
+    size_t colp = 0;
+    for (int ax = 0; ax < D - 1; ++ax) {
+        colp = std::max(colp, padded_len(a.dims[ax]));
+        maxn = std::max(maxn, (size_t)a.dims[ax]);
+    }
+    const size_t tw_b = al(maxn * elem);
+    auto row_b = [&](int r) { return (size_t)((r * S + 1) / 2) * padded_len(a.nr) * elem; };
+    auto col_b = [&](int t) { return (size_t)S * t * colp * elem; };
+    auto total = [&](size_t line) { return (two ? 2 : 1) * al(line) + tw_b; };
+    if (total(std::max(row_b(1), col_b(1))) > smem_cap) return 0;
+    // largest chunk / tile that fits
+    int rpb_max = 1;
+    while (rpb_max < a.nrows && total(std::max(row_b(rpb_max + 1), col_b(1))) <= smem_cap) ++rpb_max;
+    int tk_max = 1;
+    while (tk_max < a.nh && total(std::max(row_b(1), col_b(tk_max + 1))) <= smem_cap) ++tk_max;
+    // default: every CTA gets one chunk (row pass) and one tile (strided
+    // passes) when the grid allows it; tiles of at least two columns on
+    // larger grids, so that a tile row is a whole 32-byte sector
+    const int no = D == 2 ? 1 : std::min(a.dims[0], a.dims[1]);
+    if (rpb <= 0) rpb = (a.nrows + ncta - 1) / ncta;
+    if (tk <= 0) {
+        const int tiles = std::max(1, (ncta + no - 1) / no);  // tiles wanted per outer index
+        tk = (a.nh + tiles - 1) / tiles;
+        if ((long)a.N >= (1L << 18)) tk = std::max(tk, 2);
+    }
+    a.rpb = std::max(1, std::min(rpb, rpb_max));
+    a.tk = std::max(1, std::min(tk, tk_max));
+    const size_t line = al(std::max(row_b(a.rpb), col_b(a.tk)));
+    a.smem_half = (int)line;
+    a.tw_off = (int)((two ? 2 : 1) * line);
+    return (size_t)a.tw_off + tw_b;
 }
 
 static void lame(double E, double nu, int D, bool ps, double* lam, double* mu) {
@@ -191,38 +245,25 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     a.pixel = pixel;
     for (int i = 0; i < D; ++i)
         if (!plan_axis(dims_[i], &a.ax[i], &tw_bufs_)) throw std::invalid_argument("unsupported FFT length (prime factor > 7)");
-    // decomposition
+    // decomposition: two CTAs per SM (the kernel's register bound), each with
+    // up to half an SM's shared memory; passes tiled over every CTA
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    a.rpb = (S_ == 3) ? 2 : 1;
-    if ((long)nrows / a.rpb < nsm / 2 && a.rpb > 1) a.rpb = 1;
-    int no = (D == 2) ? 1 : std::max(dims_[0], dims_[1]);
-    a.tk = ((long)no * nh >= 4L * nsm) ? 2 : 1;
-    const int row_items = (nrows + a.rpb - 1) / a.rpb;
-    const int col_items = ((D == 2) ? 1 : std::min(dims_[0], dims_[1])) * ((nh + a.tk - 1) / a.tk);
-    // shared memory: two buffers of the largest pass
-    const size_t elem = sizeof(cplx<double>);
-    const size_t row_b = (size_t)((a.rpb * S_ + 1) / 2) * padded_len(nr) * elem;
-    size_t col_b = 0;
-    for (int ax = 0; ax < D - 1; ++ax) col_b = std::max(col_b, (size_t)S_ * a.tk * padded_len(dims_[ax]) * elem);
-    const size_t half_b = (std::max(row_b, col_b) + 127) / 128 * 128;
-    smem_ = 2 * half_b;
-    a.smem_half = (int)half_b;
-    if (smem_ > 200 * 1024) throw std::invalid_argument("grid axis too long for the shared-memory FFT");
+    smem_ = plan_passes(a, kLsCtasPerSm * nsm, kLsSmemCap);
+    if (smem_ == 0) throw std::invalid_argument("grid axis too long for the shared-memory FFT");
     // the FP64 kernel and its FP32 twin (FP32-refined solves) share one grid:
     // the smaller of their co-resident block counts
     auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
     auto kfn32 = (D == 2) ? (const void*)ls_kernel<2, float> : (const void*)ls_kernel<3, float>;
-    MGK_CK(ensure_dyn_smem(kfn, smem_));
-    MGK_CK(ensure_dyn_smem(kfn32, smem_));
+    MGK_CK(ensure_dyn_smem(kfn, kLsSmemCap));
+    MGK_CK(ensure_dyn_smem(kfn32, kLsSmemCap));
     int per_sm = 0, per_sm32 = 0;
     MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads_, smem_));
     MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, kfn32, threads_, smem_));
     per_sm = std::min(per_sm, per_sm32);
     if (per_sm < 1) throw std::runtime_error("LS kernel does not fit on an SM");
-    grid_ = std::min(std::max(row_items, col_items), per_sm * nsm);
-    grid_ = std::max(grid_, 1);
+    grid_ = std::max(1, std::min(plan_items(a), per_sm * nsm));
     // buffers
     bytes_ = 0;
     auto alloc = [&](void** p, size_t b) {
@@ -232,8 +273,8 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     alloc((void**)&d_eps_s_, sizeof(double) * S_ * N);
     alloc((void**)&d_lam_, sizeof(double) * N);
     alloc((void**)&d_mu_, sizeof(double) * N);
-    alloc(&d_spec_, elem * S_ * (size_t)nrows * nh);
-    alloc((void**)&d_partials_, sizeof(double) * kMaxPartials * grid_);
+    alloc(&d_spec_, sizeof(cplx<double>) * S_ * (size_t)nrows * a.nhs);
+    alloc((void**)&d_partials_, sizeof(double) * kMaxPartials * (grid_ + 1));
     alloc((void**)&d_res_, sizeof(LsResult));
     alloc((void**)&d_res32_, sizeof(LsResult));
     MGK_CK(cudaEventCreate(&ev0_));
@@ -250,6 +291,7 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     a.mu = d_mu_;
     a.spec = d_spec_;
     a.partials = d_partials_;
+    a.red = d_partials_ + (size_t)kMaxPartials * grid_;
     a.result = d_res_;
     a.bar = d_bar_;
     a.err = d_bar_ + 2;
@@ -500,19 +542,6 @@ __global__ void noalloc_twiddle_kernel(int n, cplx<double>* tw64, cplx<float>* t
     }
 }
 
-bool noalloc_radices(int n, FftAxis* ax) {
-    std::memset(ax, 0, sizeof(*ax));
-    ax->n = n;
-    int m = n, k = 0;
-    while (m % 8 == 0 && m >= 64 && k < kMaxStages) { ax->radix[k++] = 8; m /= 8; }
-    while (m % 4 == 0 && k < kMaxStages) { ax->radix[k++] = 4; m /= 4; }
-    static const int primes[] = {2, 3, 5, 7};
-    for (int p : primes)
-        while (m % p == 0 && k < kMaxStages) { ax->radix[k++] = p; m /= p; }
-    ax->nst = k;
-    return m == 1;
-}
-
 }  // namespace
 }  // namespace mgk
 
@@ -548,32 +577,23 @@ mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stres
     a.nr = nr;
     a.nh = nh;
     for (int i = 0; i < D; ++i)
-        if (!noalloc_radices(dims[i], &a.ax[i])) return noalloc_fail(MGK_BAD_SHAPE, "unsupported FFT length (prime factor > 7)");
+        if (!plan_radices(dims[i], &a.ax[i])) return noalloc_fail(MGK_BAD_SHAPE, "unsupported FFT length (prime factor > 7)");
+    a.N = (int)N;
+    a.nrows = (int)nrows;
     // decomposition: the same rules as LsSolver
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    a.rpb = (S == 3) ? 2 : 1;
-    if (nrows / a.rpb < nsm / 2 && a.rpb > 1) a.rpb = 1;
-    const int no = (D == 2) ? 1 : std::max(dims[0], dims[1]);
-    a.tk = ((long)no * nh >= 4L * nsm) ? 2 : 1;
-    const long row_items = (nrows + a.rpb - 1) / a.rpb;
-    const long col_items = (long)((D == 2) ? 1 : std::min(dims[0], dims[1])) * ((nh + a.tk - 1) / a.tk);
-    const size_t elem = sizeof(cplx<double>);
-    const size_t row_b = (size_t)((a.rpb * S + 1) / 2) * padded_len(nr) * elem;
-    size_t col_b = 0;
-    for (int ax = 0; ax < D - 1; ++ax) col_b = std::max(col_b, (size_t)S * a.tk * padded_len(dims[ax]) * elem);
-    const size_t half_b = (std::max(row_b, col_b) + 127) / 128 * 128;
-    const size_t smem = 2 * half_b;
-    a.smem_half = (int)half_b;
-    if (smem > 200 * 1024) return noalloc_fail(MGK_BAD_SHAPE, "grid axis too long for the shared-memory FFT");
+    const size_t smem = plan_passes(a, kLsCtasPerSm * nsm, kLsSmemCap);
+    if (smem == 0) return noalloc_fail(MGK_BAD_SHAPE, "grid axis too long for the shared-memory FFT");
     auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
-    if (ensure_dyn_smem(kfn, smem) != cudaSuccess)
+    if (ensure_dyn_smem(kfn, kLsSmemCap) != cudaSuccess)
         return noalloc_fail(MGK_CUDA_ERROR, "cannot configure the LS kernel");
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, 256, smem) != cudaSuccess || per_sm < 1)
         return noalloc_fail(MGK_CUDA_ERROR, "LS kernel does not fit on an SM");
-    const int grid = (int)std::max(1L, std::min(std::max(row_items, col_items), (long)per_sm * nsm));
+    const int grid = std::max(1, std::min(plan_items(a), per_sm * nsm));
+    const size_t elem = sizeof(cplx<double>);
     // carve the static scratch array
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -582,7 +602,7 @@ mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stres
         return o;
     };
     const size_t o_bar = take(4 * sizeof(unsigned)), o_res = take(sizeof(LsResult)), o_sum = take(16 * sizeof(double));
-    const size_t o_part = take(sizeof(double) * kMaxPartials * grid);
+    const size_t o_part = take(sizeof(double) * kMaxPartials * (grid + 1));
     size_t o_tw64[3] = {0, 0, 0}, o_tw32[3] = {0, 0, 0};
     for (int i = 0; i < D; ++i) {
         o_tw64[i] = take(sizeof(cplx<double>) * dims[i]);
@@ -590,7 +610,7 @@ mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stres
     }
     const size_t o_lam = take(sizeof(double) * N), o_mu = take(sizeof(double) * N), o_eps = take(sizeof(double) * S * N);
     const size_t o_epsp = eps_plastic_dev ? take(sizeof(double) * S * N) : 0;
-    const size_t o_spec = take(elem * S * (size_t)nrows * nh);
+    const size_t o_spec = take(elem * S * (size_t)nrows * a.nhs);
     if (off > (size_t)MGK_NOALLOC_SCRATCH_BYTES) {
         char msg[160];
         snprintf(msg, sizeof(msg), "grid needs %zu scratch bytes, above the %u-byte static limit", off,
@@ -671,6 +691,7 @@ mgk_status mgk_ls_solve_noalloc(int dim, int nx, int ny, int nz, int plane_stres
     a.mu = mu;
     a.spec = base + o_spec;
     a.partials = reinterpret_cast<double*>(base + o_part);
+    a.red = a.partials + (size_t)kMaxPartials * grid;
     a.result = reinterpret_cast<LsResult*>(base + o_res);
     a.bar = reinterpret_cast<unsigned*>(base + o_bar);
     a.err = a.bar + 2;

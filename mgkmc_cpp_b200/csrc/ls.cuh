@@ -25,6 +25,11 @@
 namespace mgk {
 
 constexpr int kMaxPartials = 16;
+// Launch shape of the one-solve kernel: 256-thread CTAs, two per SM (its
+// register bound), each with at most this much dynamic shared memory (two
+// such CTAs and their static shared memory fit an SM's 228 KB).
+constexpr int kLsCtasPerSm = 2;
+constexpr size_t kLsSmemCap = 104 * 1024;
 // relative-change target of the FP32 phase of an FP32-refined solve: above
 // the FP32 rounding floor of the iteration (~1e-7 relative)
 constexpr double kFp32Tol = 1e-6;
@@ -41,6 +46,7 @@ struct LsArgs {
     int D, S;
     int dims[3];
     int N, nr, nh, nrows;  // voxels, contiguous-axis length, its half spectrum, rows = N / nr
+    int nhs;               // spectrum row stride (nh rounded up to 4: 32-byte aligned rows)
     int rpb;               // rows per row-pass chunk
     int tk;                // columns per strided-pass tile
     int max_iter;
@@ -50,7 +56,8 @@ struct LsArgs {
     double norm_extra;     // 2 N sum_offdiag w^2: antisymmetric part of |eps|^2 (uniform field)
     double norm_extra_first;  // same for the first iteration (warm start of a non-uniform field)
     double diff_extra_first;  // antisymmetric part of |eps_new - eps|^2 in the first iteration
-    int smem_half;         // byte offset of the second shared-memory buffer
+    int smem_half;         // byte offset of the second line buffer
+    int tw_off;            // byte offset of the shared-memory twiddle table
     double ebar_s[6];      // symmetric part of the prescribed mean strain
     double lam0, mu0, inv2mu0, bcoef;
     double pixel;
@@ -59,8 +66,9 @@ struct LsArgs {
     const double* epsp_s;  // S x N or null
     const double* lam;     // N
     const double* mu;      // N
-    void* spec;            // S x nrows x nh complex (T)
+    void* spec;            // S x nrows x nhs complex (T)
     double* partials;      // gridDim.x x kMaxPartials
+    double* red;           // kMaxPartials: the reduced partials (written by the last CTA of a barrier)
     LsResult* result;
     unsigned* bar;
     unsigned* err;
@@ -155,5 +163,19 @@ private:
 // Plans the radix sequence of a length-n transform (radix-8 while n >= 64,
 // radix-4, then 2, 3, 5, 7).  Returns false for lengths with other prime factors.
 bool plan_axis(int n, FftAxis* ax, std::vector<void*>* owned);
+// The radices alone (no twiddle tables); false for unsupported lengths.
+bool plan_radices(int n, FftAxis* ax);
+
+// Pass tiling of one solve run by ncta CTAs whose dynamic shared memory may
+// not exceed smem_cap bytes: rows per row chunk (rpb) and columns per strided
+// tile (tk) spread the work over the CTAs (a 0 argument picks them; given
+// values are clamped to what fits), and the shared-memory layout (line
+// buffer, second buffer for axes longer than kWarpFftMax, twiddle table).
+// Needs a.D, a.S, a.dims, a.N, a.nr, a.nh, a.nrows and the axes' radices.
+// Returns the dynamic shared-memory bytes of a launch, 0 when nothing fits.
+size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, int rpb = 0, int tk = 0);
+// Work items of a plan: the larger of the row chunks and the column tiles
+// (a CTA beyond it idles in every pass).
+int plan_items(const LsArgs& a);
 
 }  // namespace mgk

@@ -97,35 +97,67 @@ MGK_DEV void green_apply(const double* q, const bool* nyq, cplx<T>* t, double in
     for (int c = 0; c < S; ++c) t[c] = {T(0.5) * (t0[c].x + t1[c].x), T(0.5) * (t0[c].y + t1[c].y)};
 }
 
+MGK_DEV void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// Shared-memory layout of a pass: the two line buffers at 0 and smem_half,
+// the axis twiddle table at tw_off.
+template <typename T>
+struct PassSmem {
+    cplx<T>* buf0;
+    cplx<T>* buf1;
+    cplx<T>* tw;
+};
+template <typename T>
+MGK_DEV PassSmem<T> pass_smem(const LsArgs& a, unsigned char* smem) {
+    return {reinterpret_cast<cplx<T>*>(smem), reinterpret_cast<cplx<T>*>(smem + a.smem_half),
+            reinterpret_cast<cplx<T>*>(smem + a.tw_off)};
+}
+
 // Row pass along the contiguous axis.  MODE 0 (prologue): set the field (warm
 // shift or fill), build tau, forward transform.  MODE 1 (iteration): inverse
 // transform of the Green-filtered spectrum, strain update with norms and
-// macro sums, then tau of the new field and its forward transform.
+// macro sums, then tau of the new field and its forward transform.  A chunk
+// of rpb rows holds its S * rpb real lines packed two per complex line; the
+// transforms are warp-owned (fft_any), so a chunk needs four CTA barriers.
 template <int D, typename T, int MODE>
-MGK_DEV void row_pass(const LsArgs& a, int cta, int ncta, cplx<T>* buf0, cplx<T>* buf1, double* part, const double* shift) {
+MGK_DEV void row_pass(const LsArgs& a, int cta, int ncta, unsigned char* smem, double* part, const double* shift) {
     constexpr int S = D == 2 ? 3 : 6;
     const int n = a.nr, nh = a.nh, N = a.N;
     cplx<T>* spec = reinterpret_cast<cplx<T>*>(a.spec);
-    const long cs = (long)a.nrows * nh;
+    const long cs = (long)a.nrows * a.nhs;
     const int nchunks = (a.nrows + a.rpb - 1) / a.rpb;
     const FftAxis& ax = a.ax[D - 1];
     const int lsn = pad_len(n);
+    const PassSmem<T> sm = pass_smem<T>(a, smem);
+    load_twiddles<T>(ax, sm.tw);
     for (int ch = cta; ch < nchunks; ch += ncta) {
         const int row0 = ch * a.rpb;
         const int rows = min(a.rpb, a.nrows - row0);
         const int L = rows * S;        // real lines in this chunk
         const int P = (L + 1) >> 1;    // packed complex lines
-        cplx<T>* z = buf0;
-        cplx<T>* other = buf1;
+        const long v0 = (long)row0 * n;
+        cplx<T>* z = sm.buf0;
+        cplx<T>* other = sm.buf1;
         if (MODE == 1) {
+            // the update's operands go to L1 while the spectrum is loaded and
+            // transformed (the chunk's rows are contiguous in every array)
+            for (int o = threadIdx.x * 16; o < rows * n; o += blockDim.x * 16) {
+#pragma unroll
+                for (int c = 0; c < S; ++c) {
+                    prefetch_l1(a.eps_s + (long)c * N + v0 + o);
+                    if (a.epsp_s) prefetch_l1(a.epsp_s + (long)c * N + v0 + o);
+                }
+                prefetch_l1(a.lam + v0 + o);
+                prefetch_l1(a.mu + v0 + o);
+            }
             for (int idx = threadIdx.x; idx < P * n; idx += blockDim.x) {
                 const int p = idx / n, k = idx - p * n;
                 const bool hi = 2 * k > n;
                 const int kk = hi ? n - k : k;
                 const int la = 2 * p, lb = 2 * p + 1;
-                cplx<T> A = spec[(la % S) * cs + (long)(row0 + la / S) * nh + kk];
+                cplx<T> A = spec[(la % S) * cs + (long)(row0 + la / S) * a.nhs + kk];
                 cplx<T> B = {T(0), T(0)};
-                if (lb < L) B = spec[(lb % S) * cs + (long)(row0 + lb / S) * nh + kk];
+                if (lb < L) B = spec[(lb % S) * cs + (long)(row0 + lb / S) * a.nhs + kk];
                 if (hi) {
                     A = cconj(A);
                     B = cconj(B);
@@ -133,13 +165,13 @@ MGK_DEV void row_pass(const LsArgs& a, int cta, int ncta, cplx<T>* buf0, cplx<T>
                 z[p * lsn + pad_idx(k)] = {A.x - B.y, A.y + B.x};
             }
             __syncthreads();
-            z = fft_lines<T>(buf0, buf1, P, ax, +1);
-            other = (z == buf0) ? buf1 : buf0;
+            z = fft_any<T>(sm.buf0, sm.buf1, P, ax, sm.tw, +1);
+            other = (z == sm.buf0) ? sm.buf1 : sm.buf0;
             __syncthreads();
         }
         for (int idx = threadIdx.x; idx < rows * n; idx += blockDim.x) {
             const int r = idx / n, y = idx - r * n;
-            const long v = (long)(row0 + r) * n + y;
+            const long v = v0 + idx;
             double sn[S];
 #pragma unroll
             for (int c = 0; c < S; ++c) {
@@ -185,7 +217,7 @@ MGK_DEV void row_pass(const LsArgs& a, int cta, int ncta, cplx<T>* buf0, cplx<T>
             }
         }
         __syncthreads();
-        cplx<T>* Z = fft_lines<T>(z, other, P, ax, -1);
+        cplx<T>* Z = fft_any<T>(z, other, P, ax, sm.tw, -1);
         __syncthreads();
         for (int idx = threadIdx.x; idx < P * nh; idx += blockDim.x) {
             const int p = idx / nh, k = idx - p * nh;
@@ -193,10 +225,10 @@ MGK_DEV void row_pass(const LsArgs& a, int cta, int ncta, cplx<T>* buf0, cplx<T>
             const cplx<T> zm = cconj(Z[p * lsn + pad_idx(k == 0 ? 0 : n - k)]);
             const int la = 2 * p, lb = 2 * p + 1;
             const cplx<T> A = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y + zm.y)};
-            spec[(la % S) * cs + (long)(row0 + la / S) * nh + k] = A;
+            spec[(la % S) * cs + (long)(row0 + la / S) * a.nhs + k] = A;
             if (lb < L) {
                 const cplx<T> B = {T(0.5) * (zk.y - zm.y), T(-0.5) * (zk.x - zm.x)};
-                spec[(lb % S) * cs + (long)(row0 + lb / S) * nh + k] = B;
+                spec[(lb % S) * cs + (long)(row0 + lb / S) * a.nhs + k] = B;
             }
         }
         __syncthreads();
@@ -207,20 +239,20 @@ MGK_DEV void row_pass(const LsArgs& a, int cta, int ncta, cplx<T>* buf0, cplx<T>
 // adjacent half-spectrum columns.  KIND 0: forward only; 1: inverse only;
 // 2: forward, Green operator, inverse (the last non-contiguous axis, x).
 template <int D, typename T, int KIND>
-MGK_DEV void strided_pass(const LsArgs& a, int cta, int ncta, int axis, cplx<T>* buf0, cplx<T>* buf1) {
+MGK_DEV void strided_pass(const LsArgs& a, int cta, int ncta, int axis, unsigned char* smem) {
     constexpr int S = D == 2 ? 3 : 6;
     const int nh = a.nh;
     const int n = a.dims[axis];
     cplx<T>* spec = reinterpret_cast<cplx<T>*>(a.spec);
-    const long cs = (long)a.nrows * nh;
+    const long cs = (long)a.nrows * a.nhs;
     long st, os;
     int no;
     if (D == 2) {
-        st = nh; no = 1; os = 0;
+        st = a.nhs; no = 1; os = 0;
     } else if (axis == 1) {
-        st = nh; no = a.dims[0]; os = (long)a.dims[1] * nh;
+        st = a.nhs; no = a.dims[0]; os = (long)a.dims[1] * a.nhs;
     } else {
-        st = (long)a.dims[1] * nh; no = a.dims[1]; os = nh;
+        st = (long)a.dims[1] * a.nhs; no = a.dims[1]; os = a.nhs;
     }
     const int tk = a.tk;
     const int ntk = (nh + tk - 1) / tk;
@@ -228,6 +260,8 @@ MGK_DEV void strided_pass(const LsArgs& a, int cta, int ncta, int axis, cplx<T>*
     const int nl = S * tk;
     const FftAxis& fx = a.ax[axis];
     const int lsn = pad_len(n);
+    const PassSmem<T> sm = pass_smem<T>(a, smem);
+    load_twiddles<T>(fx, sm.tw);
     for (int it = cta; it < items; it += ncta) {
         const int o = it / ntk;
         const int k0 = (it - o * ntk) * tk;
@@ -237,10 +271,10 @@ MGK_DEV void strided_pass(const LsArgs& a, int cta, int ncta, int axis, cplx<T>*
             const int t = idx % tk;
             const int i = (idx / tk) % n;
             const int c = idx / (tk * n);
-            buf0[(c * tk + t) * lsn + pad_idx(i)] = (t < tku) ? spec[c * cs + base + t + i * st] : cplx<T>{T(0), T(0)};
+            sm.buf0[(c * tk + t) * lsn + pad_idx(i)] = (t < tku) ? spec[c * cs + base + t + i * st] : cplx<T>{T(0), T(0)};
         }
         __syncthreads();
-        cplx<T>* Z = fft_lines<T>(buf0, buf1, nl, fx, KIND == 1 ? +1 : -1);
+        cplx<T>* Z = fft_any<T>(sm.buf0, sm.buf1, nl, fx, sm.tw, KIND == 1 ? +1 : -1);
         __syncthreads();
         if (KIND == 2) {
             for (int idx = threadIdx.x; idx < tku * n; idx += blockDim.x) {
@@ -268,8 +302,8 @@ MGK_DEV void strided_pass(const LsArgs& a, int cta, int ncta, int axis, cplx<T>*
                 for (int c = 0; c < S; ++c) Z[(c * tk + t) * lsn + pad_idx(kx)] = tv[c];
             }
             __syncthreads();
-            cplx<T>* other = (Z == buf0) ? buf1 : buf0;
-            Z = fft_lines<T>(Z, other, nl, fx, +1);
+            cplx<T>* other = (Z == sm.buf0) ? sm.buf1 : sm.buf0;
+            Z = fft_any<T>(Z, other, nl, fx, sm.tw, +1);
             __syncthreads();
         }
         for (int idx = threadIdx.x; idx < nl * n; idx += blockDim.x) {
@@ -289,32 +323,76 @@ MGK_DEV void publish_partials(const LsArgs& a, int cta, double* part, double* re
         for (int k = 0; k < NP; ++k) a.partials[cta * kMaxPartials + k] = part[k];
 }
 
-// Every CTA reduces all partials in the same fixed order -> identical values.
-// 256 threads: thread t sums value (t & 15) over blocks (t >> 4), (t >> 4) + 16, ...;
-// then the 16 group sums are added in group order.
+// Group barrier that also sums the CTAs' partials (publish_partials): the last
+// CTA to arrive adds them in a fixed order -- thread t sums value (t & 15)
+// over CTAs (t >> 4), (t >> 4) + 16, ..., then the 16 group sums are added
+// in group order, the same bits whichever CTA arrives last -- writes the sums
+// to a.red and releases the others, which read them there.  `out` (shared,
+// NP values) gets the sums in every CTA.  256 threads per CTA.  Bounded like
+// grid_sync; returns false when a wait gave up.
 template <int NP>
-MGK_DEV void gather_partials(const LsArgs& a, int ncta, double* out /* shared, NP */) {
+MGK_DEV bool grid_sync_reduce(const LsArgs& a, const GridBar& g, int ncta, double* out) {
     __shared__ double grp[256];
-    const int k = threadIdx.x & 15, g = threadIdx.x >> 4;
-    double s = 0.0;
-    if (k < NP) {
-#pragma unroll 4
-        for (int b = g; b < ncta; b += 16) s += __ldcg(&a.partials[b * kMaxPartials + k]);
-    }
-    grp[threadIdx.x] = s;
+    __shared__ int s_last, s_ok;
+    __shared__ unsigned s_gen;
     __syncthreads();
-    if (threadIdx.x < NP) {
-        double t = 0.0;
-        for (int gg = 0; gg < 16; ++gg) t += grp[gg * 16 + threadIdx.x];
-        out[threadIdx.x] = t;
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = g.bar + 1;
+        s_gen = *gen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(g.bar, 1u);
+        s_last = arrived == g.nblocks - 1;
+        s_ok = 1;
     }
     __syncthreads();
+    if (s_last) {
+        const int k = threadIdx.x & 15, gg = threadIdx.x >> 4;
+        double sum = 0.0;
+        if (k < NP)
+            for (int b = gg; b < ncta; b += 16) sum += __ldcg(&a.partials[b * kMaxPartials + k]);
+        grp[threadIdx.x] = sum;
+        __syncthreads();
+        if (threadIdx.x < NP) {
+            double t = 0.0;
+            for (int q = 0; q < 16; ++q) t += grp[q * 16 + threadIdx.x];
+            __stcg(&a.red[threadIdx.x], t);
+            out[threadIdx.x] = t;
+            __threadfence();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            atomicExch(g.bar, 0u);
+            __threadfence();
+            atomicAdd(g.bar + 1, 1u);
+        }
+    } else {
+        if (threadIdx.x == 0) {
+            volatile unsigned* gen = g.bar + 1;
+            const unsigned long long t0 = global_ns();
+            unsigned polls = 0;
+            while (*gen == s_gen) {
+                __nanosleep(32);
+                if ((*(volatile unsigned*)g.err & MGK_DERR_BARRIER_TIMEOUT) ||
+                    ((++polls & 255u) == 0 && global_ns() - t0 > g.limit_ns)) {
+                    atomicOr(g.err, MGK_DERR_BARRIER_TIMEOUT);
+                    s_ok = 0;
+                    break;
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        if (s_ok && threadIdx.x < NP) out[threadIdx.x] = __ldcg(&a.red[threadIdx.x]);
+    }
+    if (threadIdx.x == 0 && (*(volatile unsigned*)g.err & MGK_DERR_BARRIER_TIMEOUT)) s_ok = 0;
+    __syncthreads();
+    return s_ok != 0;
 }
 
 // One LS solve by a group of ncta co-resident CTAs (rank cta), synchronised by
-// the bounded barrier `gb`; smem_raw is the CTA's dynamic shared memory
-// (2 x a.smem_half bytes).  The result goes to a.result.  Returns false when a
-// barrier wait gave up (the error word is set).
+// the bounded barrier `gb`; smem_raw is the CTA's dynamic shared memory (the
+// pass layout of pass_smem).  The result goes to a.result.  Returns false
+// when a barrier wait gave up (the error word is set).
 template <int D, typename T>
 MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& gb, unsigned char* smem_raw) {
     constexpr int S = D == 2 ? 3 : 6;
@@ -322,8 +400,6 @@ MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& g
     __shared__ double red[14 * 32];
     __shared__ double vals[14];
     __shared__ double s_shift[6];
-    cplx<T>* buf0 = reinterpret_cast<cplx<T>*>(smem_raw);
-    cplx<T>* buf1 = reinterpret_cast<cplx<T>*>(smem_raw + a.smem_half);
     // fault injection (set from the host for tests): this CTA never arrives,
     // so the others' bounded waits run out and they return with the error set
     if (a.test_absent == cta + 1) return false;
@@ -341,40 +417,36 @@ MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& g
                 for (int c = 0; c < S; ++c) acc[c] += a.eps_s[(long)c * a.N + v];
         }
         publish_partials<NP>(a, cta, acc, red);
-        if (!grid_sync(gb)) return false;
-        gather_partials<NP>(a, ncta, vals);
+        if (!grid_sync_reduce<NP>(a, gb, ncta, vals)) return false;
         if (threadIdx.x < S) s_shift[threadIdx.x] = a.ebar_s[threadIdx.x] - vals[threadIdx.x] * a.inv_n;
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < S; ++c) shift[c] = s_shift[c];
-        if (!grid_sync(gb)) return false;
     }
     double part[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) part[k] = 0.0;
-    row_pass<D, T, 0>(a, cta, ncta, buf0, buf1, part, shift);
+    row_pass<D, T, 0>(a, cta, ncta, smem_raw, part, shift);
     publish_partials<NP>(a, cta, part, red);
-    if (!grid_sync(gb)) return false;
-    gather_partials<NP>(a, ncta, vals);
+    if (!grid_sync_reduce<NP>(a, gb, ncta, vals)) return false;
     int it = 0;
     double diff = 0.0;
     while (it < a.max_iter) {
         if (D == 3) {
-            strided_pass<D, T, 0>(a, cta, ncta, 1, buf0, buf1);
+            strided_pass<D, T, 0>(a, cta, ncta, 1, smem_raw);
             if (!grid_sync(gb)) return false;
         }
-        strided_pass<D, T, 2>(a, cta, ncta, 0, buf0, buf1);
+        strided_pass<D, T, 2>(a, cta, ncta, 0, smem_raw);
         if (!grid_sync(gb)) return false;
         if (D == 3) {
-            strided_pass<D, T, 1>(a, cta, ncta, 1, buf0, buf1);
+            strided_pass<D, T, 1>(a, cta, ncta, 1, smem_raw);
             if (!grid_sync(gb)) return false;
         }
 #pragma unroll
         for (int k = 0; k < NP; ++k) part[k] = 0.0;
-        row_pass<D, T, 1>(a, cta, ncta, buf0, buf1, part, shift);
+        row_pass<D, T, 1>(a, cta, ncta, smem_raw, part, shift);
         publish_partials<NP>(a, cta, part, red);
-        if (!grid_sync(gb)) return false;
-        gather_partials<NP>(a, ncta, vals);
+        if (!grid_sync_reduce<NP>(a, gb, ncta, vals)) return false;
         const double dx = it == 0 ? a.diff_extra_first : 0.0;
         const double nx = it == 0 ? a.norm_extra_first : a.norm_extra;
         ++it;
