@@ -87,7 +87,9 @@ def make(name, rd):
     E = np.asarray(cfg.E, dtype=np.float64).reshape(-1)
     out = compact(res, cfg, E)
     out.update(workload=np.array(wl), seed=seed, events=nev)
-    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    tmp = os.path.join(HERE, name + ".tmp.npz")
+    np.savez_compressed(tmp, **out)
+    os.replace(tmp, os.path.join(HERE, name + ".npz"))  # never a half-written fixture
     kinds = np.bincount(res["trace"][:, 0].astype(int), minlength=4)
     print("wrote %s: %d rows (kinds %s), %d flipped voxels, reference %.1f s" % (name, len(res["trace"]), kinds,
                                                                                   len(out["flip_vox"]), dt), flush=True)
