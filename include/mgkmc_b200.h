@@ -104,7 +104,7 @@ MGK_API void mgk_ls_destroy(mgk_ls* h);
  * refused with MGK_BAD_SHAPE.  The intermediates take about 88 bytes per voxel
  * in 2D and 170 in 3D with a plastic strain (64 and 112 without), so the limit
  * is about 190k voxels in 2D and 98k in 3D: 432x432 fits and 448x432 does not
- * (2D with a plastic strain); 44^3 fits and 48^3 does not (3D).  Every call
+ * (2D with a plastic strain); 45^3 fits and 48^3 does not (3D).  Every call
  * looks up the array's device address on the current device (the first one
  * may load the library's GPU code), so make the first call before any stream
  * capture.  All calls share the one array, which

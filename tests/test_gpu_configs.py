@@ -4,7 +4,8 @@ by the reference itself (tests/golden/make_golden_configs.py):
 * cfg0_homog2d_32       2D 32^2 homogeneous, M = 18, seed 0, 2000 thermal events
 * cfg1_hetero2d_256_s*  2D 256^2 lognormal E (CoV 0.1), M = 18, seeds 0-3, 100 events
                         (the benchmark's four-replica launch in the batched form)
-* cfg2_hetero3d_64      3D 64^3 lognormal E (CoV 0.15), M = 100 random 3D modes, 20 events
+* cfg2_hetero3d_64      3D 64^3 lognormal E (CoV 0.15), M = 100 random 3D modes
+                        (gamma0 0.03), 20 events
 * ens2d_512_s32, ens3d_96_s58   one 512^2 and one 96^3 replica of the ensemble, 20 events
 
 Bar, as in the small golden cases: event kinds, selected modes and cascade
@@ -43,6 +44,14 @@ def inputs(g, tmp_path):
     assert abs(E.sum() - float(g["E_sum"])) <= 1e-13 * abs(float(g["E_sum"]))
     assert abs((E * E).sum() - float(g["E_sq"])) <= 1e-13 * abs(float(g["E_sq"]))
     return cfg
+
+
+def clock_rtol(cfg):
+    """The simulation clock is a sum of waits -ln(u1)/R; the reference sums the
+    NM rates of R left to right in FP64, an error that grows like sqrt(NM)
+    ulps (about 6e-12 at 96^3 x 100 modes), against this build's nearly exact
+    double-double sum."""
+    return max(1e-12, 2e-15 * np.sqrt(cfg.n_voxels * cfg.M))
 
 
 def check_fields(g, cfg, eps, sig, epsp, cat, Q0, exact):
@@ -86,11 +95,13 @@ def test_plain_form_at_config(G, name, tmp_path):
     g = golden(name)
     cfg = inputs(g, tmp_path)
     sim, tr = run_plain(G, cfg, int(g["events"]), tmp_path)
-    compare_trace(tr, g["trace"], tol=1e-9)
+    N = cfg.n_voxels
+    compare_trace(tr, g["trace"], tol=1e-9, eps_floor=np.sqrt(float(g["eps_sq"]) / N),
+                  sig_floor=np.sqrt(float(g["sig_sq"]) / N))
     check_fields(g, cfg, sim.eps_field, sim.sig_field, sim.eps_plastic, sim.catalog, sim.Q0, exact=True)
     D = cfg.dim
     m = sim.macro()
-    assert abs(m[2 * D * D] - g["macro"][-1]) <= 1e-12 * abs(g["macro"][-1])  # simulation clock
+    assert abs(m[2 * D * D] - g["macro"][-1]) <= clock_rtol(cfg) * abs(g["macro"][-1])  # simulation clock
 
 
 def check_batch_replica(b, r, g, cfg):
@@ -105,7 +116,7 @@ def check_batch_replica(b, r, g, cfg):
                  b.field(r, "catalog"), b.field(r, "Q0"), exact=False)
     D = cfg.dim
     m = b.macro(r)
-    assert abs(m[2 * D * D] - g["macro"][-1]) <= 1e-12 * abs(g["macro"][-1])
+    assert abs(m[2 * D * D] - g["macro"][-1]) <= clock_rtol(cfg) * abs(g["macro"][-1])
 
 
 @pytest.mark.parametrize("name", SINGLE)

@@ -124,7 +124,7 @@ def test_noalloc_refuses_grids_beyond_its_static_scratch(env):
     torch, G, L = env
     # 16 MiB of scratch: just below the limit, 2D with a plastic strain and 3D
     assert _noalloc_status(env, (432, 432), True) in (0, 1)
-    assert _noalloc_status(env, (44, 44, 44), True) in (0, 1)
+    assert _noalloc_status(env, (45, 45, 45), True) in (0, 1)
     # just above it, and far above it
     for dims, plastic in (((448, 432), True), ((48, 48, 48), True), ((512, 512), False)):
         assert _noalloc_status(env, dims, plastic) == 2  # MGK_BAD_SHAPE
