@@ -1046,10 +1046,11 @@ void BatchEngine::init() {
     std::vector<LsArgs> plans(n);
     smem_ = std::max((size_t)4096 * 12, kRedrawSmem);
     for (int r = 0; r < n; ++r) {
-        // the LS pass tiling re-planned for the replica's group: chunks and
-        // tiles as large as the budget allows while every CTA has work
+        // the LS pass plan for the replica's group, measured on the
+        // replica's own grid at the group's CTA count (LsSolver::tune)
         plans[r] = eng_[r]->ls_->args_;
-        const size_t need = plan_passes(plans[r], ncta_[r], ls_budget);
+        const LsPlan lp = LsSolver::autotune_enabled() ? eng_[r]->ls_->tune(ncta_[r], ls_budget) : LsPlan();
+        const size_t need = plan_passes(plans[r], ncta_[r], ls_budget, lp);
         if (need == 0) throw std::invalid_argument("grid axis too long for the batched LS passes");
         smem_ = std::max(smem_, need);
     }

@@ -22,7 +22,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -148,9 +150,15 @@ int plan_items(const LsArgs& a) {
     return std::max(row_items, col_items);
 }
 
-size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, int rpb, int tk) {
+size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, LsPlan plan) {
     const int D = a.D, S = a.S;
     ncta = std::max(ncta, 1);
+    int rpb = plan.rpb, tk = plan.tk;
+    const int path = plan.path < 0 ? (D == 2 ? 1 : 0) : plan.path;
+    for (int ax = 0; ax < D; ++ax) {
+        a.ax[ax].lw = 0;
+        if (path == 0) a.ax[ax].lw = warp_lines(a.ax[ax]);
+    }
     a.nhs = (a.nh + 3) / 4 * 4;
     const size_t elem = sizeof(cplx<double>);  // the FP32 kernel uses half of it
     auto al = [](size_t b) { return (b + 127) / 128 * 128; };
@@ -175,7 +183,7 @@ size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, int rpb, int tk) {
     // passes) when the grid allows it; tiles of at least two columns on
     // larger grids, so that a tile row is a whole 32-byte sector
     const int no = D == 2 ? 1 : std::min(a.dims[0], a.dims[1]);
-    if (rpb <= 0) rpb = (a.nrows + ncta - 1) / ncta;
+    if (rpb <= 0) rpb = std::max((a.nrows + ncta - 1) / ncta, D == 2 ? 2 : 1);
     if (tk <= 0) {
         const int tiles = std::max(1, (ncta + no - 1) / no);  // tiles wanted per outer index
         tk = (a.nh + tiles - 1) / tiles;
@@ -247,24 +255,16 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
         if (!plan_axis(dims_[i], &a.ax[i], &tw_bufs_)) throw std::invalid_argument("unsupported FFT length (prime factor > 7)");
     // decomposition: two CTAs per SM (the kernel's register bound), each with
     // up to half an SM's shared memory; passes tiled over every CTA
-    int dev = 0, nsm = 148;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    smem_ = plan_passes(a, kLsCtasPerSm * nsm, kLsSmemCap);
-    if (smem_ == 0) throw std::invalid_argument("grid axis too long for the shared-memory FFT");
-    // the FP64 kernel and its FP32 twin (FP32-refined solves) share one grid:
-    // the smaller of their co-resident block counts
+    cudaDeviceGetAttribute(&nsm_, cudaDevAttrMultiProcessorCount, dev);
+    if (plan_passes(a, kLsCtasPerSm * nsm_, kLsSmemCap) == 0)
+        throw std::invalid_argument("grid axis too long for the shared-memory FFT");
     auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
     auto kfn32 = (D == 2) ? (const void*)ls_kernel<2, float> : (const void*)ls_kernel<3, float>;
     MGK_CK(ensure_dyn_smem(kfn, kLsSmemCap));
     MGK_CK(ensure_dyn_smem(kfn32, kLsSmemCap));
-    int per_sm = 0, per_sm32 = 0;
-    MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads_, smem_));
-    MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, kfn32, threads_, smem_));
-    per_sm = std::min(per_sm, per_sm32);
-    if (per_sm < 1) throw std::runtime_error("LS kernel does not fit on an SM");
-    grid_ = std::max(1, std::min(plan_items(a), per_sm * nsm));
-    // buffers
+    // buffers (the partial sums sized for the largest grid any plan launches)
     bytes_ = 0;
     auto alloc = [&](void** p, size_t b) {
         MGK_CK(cudaMalloc(p, b));
@@ -274,7 +274,7 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     alloc((void**)&d_lam_, sizeof(double) * N);
     alloc((void**)&d_mu_, sizeof(double) * N);
     alloc(&d_spec_, sizeof(cplx<double>) * S_ * (size_t)nrows * a.nhs);
-    alloc((void**)&d_partials_, sizeof(double) * kMaxPartials * (grid_ + 1));
+    alloc((void**)&d_partials_, sizeof(double) * kMaxPartials * (kLsCtasPerSm * nsm_ + 1));
     alloc((void**)&d_res_, sizeof(LsResult));
     alloc((void**)&d_res32_, sizeof(LsResult));
     MGK_CK(cudaEventCreate(&ev0_));
@@ -291,10 +291,126 @@ LsSolver::LsSolver(int D, const int* dims, bool plane_stress, double pixel, cons
     a.mu = d_mu_;
     a.spec = d_spec_;
     a.partials = d_partials_;
-    a.red = d_partials_ + (size_t)kMaxPartials * grid_;
     a.result = d_res_;
     a.bar = d_bar_;
     a.err = d_bar_ + 2;
+    set_plan(autotune_enabled() ? tune(kLsCtasPerSm * nsm_, kLsSmemCap) : LsPlan());
+}
+
+bool LsSolver::autotune_enabled() {
+    const char* e = std::getenv("MGK_LS_AUTOTUNE");
+    return !(e && e[0] == '0');
+}
+
+void LsSolver::set_plan(const LsPlan& p) {
+    LsArgs& a = args_;
+    smem_ = plan_passes(a, kLsCtasPerSm * nsm_, kLsSmemCap, p);
+    if (smem_ == 0) throw std::invalid_argument("grid axis too long for the shared-memory FFT");
+    auto kfn = (D_ == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
+    auto kfn32 = (D_ == 2) ? (const void*)ls_kernel<2, float> : (const void*)ls_kernel<3, float>;
+    // the FP64 kernel and its FP32 twin (FP32-refined solves) share one grid:
+    // the smaller of their co-resident block counts
+    int per_sm = 0, per_sm32 = 0;
+    MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads_, smem_));
+    MGK_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, kfn32, threads_, smem_));
+    per_sm = std::min(per_sm, per_sm32);
+    if (per_sm < 1) throw std::runtime_error("LS kernel does not fit on an SM");
+    grid_ = std::max(1, std::min(plan_items(a), per_sm * nsm_));
+    a.red = d_partials_ + (size_t)kMaxPartials * grid_;
+    plan_ = LsPlan{a.rpb, a.tk, p.path < 0 ? (D_ == 2 ? 1 : 0) : p.path};
+}
+
+LsPlan LsSolver::tune(int ncta, size_t smem_cap) {
+    static std::mutex mu;
+    static std::map<std::string, LsPlan> cache;
+    char key[160];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    snprintf(key, sizeof(key), "%d:%d:%dx%dx%d:%d:%zu:%d", dev, D_, dims_[0], dims_[1], dims_[2], ncta, smem_cap,
+             (int)plane_stress_);
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    const int D = D_, S = S_;
+    auto kfn = (D == 2) ? (const void*)ls_kernel<2, double> : (const void*)ls_kernel<3, double>;
+    auto kfn32 = (D == 2) ? (const void*)ls_kernel<2, float> : (const void*)ls_kernel<3, float>;
+    // candidates: both FFT paths, row chunks of 1x, 2x, 4x the one-per-CTA
+    // size, column tiles of 1x and 2x the default width
+    LsArgs base = args_;
+    plan_passes(base, ncta, smem_cap, LsPlan{0, 0, 0});
+    const int r0 = std::max(1, (base.nrows + ncta - 1) / ncta), t0 = base.tk;
+    std::vector<LsPlan> cands;
+    for (int path = 0; path < 2; ++path)
+        for (int rm : {1, 2, 4})
+            for (int tm : {1, 2}) {
+                LsArgs t = args_;
+                if (plan_passes(t, ncta, smem_cap, LsPlan{r0 * rm, t0 * tm, path}) == 0) continue;
+                LsPlan c{t.rpb, t.tk, path};
+                bool dup = false;
+                for (const LsPlan& q : cands) dup |= q.rpb == c.rpb && q.tk == c.tk && q.path == c.path;
+                if (!dup) cands.push_back(c);
+            }
+    // scratch state: the solver's own fields stay untouched
+    double *eps = nullptr, *part = nullptr;
+    LsResult* res = nullptr;
+    unsigned* bar = nullptr;
+    LsPlan best = LsPlan();
+    float best_ms = 1e30f;
+    if (cudaMalloc(&eps, sizeof(double) * S * N_) == cudaSuccess &&
+        cudaMalloc(&part, sizeof(double) * kMaxPartials * (ncta + 1)) == cudaSuccess &&
+        cudaMalloc(&res, sizeof(LsResult)) == cudaSuccess && cudaMalloc(&bar, sizeof(unsigned) * 4) == cudaSuccess) {
+        for (const LsPlan& c : cands) {
+            LsArgs t = args_;
+            const size_t sm = plan_passes(t, ncta, smem_cap, c);
+            int per_sm = 0, per_sm32 = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads_, sm) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, kfn32, threads_, sm) != cudaSuccess)
+                continue;
+            const int grid = std::min({plan_items(t), std::min(per_sm, per_sm32) * nsm_, ncta});
+            if (grid < 1) continue;
+            t.eps_s = eps;
+            t.epsp_s = nullptr;
+            t.partials = part;
+            t.red = part + (size_t)kMaxPartials * grid;
+            t.result = res;
+            t.bar = bar;
+            t.err = bar + 2;
+            t.warm = 0;
+            t.max_iter = 3;
+            t.tol = 0.0;
+            t.norm_extra = t.norm_extra_first = t.diff_extra_first = 0.0;
+            for (int k = 0; k < 6; ++k) t.ebar_s[k] = k == 0 ? 1e-3 : (k < D ? -3e-4 : 0.0);
+            void* prm[] = {&t};
+            float ms = 1e30f;
+            bool ok = true;
+            for (int rep = 0; rep < 2 && ok; ++rep) {
+                ok = cudaMemsetAsync(bar, 0, sizeof(unsigned) * 4, stream_) == cudaSuccess;
+                ok = ok && cudaEventRecord(ev0_, stream_) == cudaSuccess;
+                ok = ok && cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(threads_), prm, sm, stream_) == cudaSuccess;
+                ok = ok && cudaEventRecord(ev1_, stream_) == cudaSuccess;
+                ok = ok && cudaStreamSynchronize(stream_) == cudaSuccess;
+                float m = 0.f;
+                if (ok && rep == 1 && cudaEventElapsedTime(&m, ev0_, ev1_) == cudaSuccess) ms = m;
+            }
+            unsigned err = 0;
+            if (ok) cudaMemcpy(&err, bar + 2, sizeof(unsigned), cudaMemcpyDeviceToHost);
+            if (!ok || err) {
+                cudaGetLastError();
+                continue;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+    }
+    cudaFree(eps);
+    cudaFree(part);
+    cudaFree(res);
+    cudaFree(bar);
+    cudaGetLastError();
+    cache[key] = best;
+    return best;
 }
 
 LsSolver::~LsSolver() {

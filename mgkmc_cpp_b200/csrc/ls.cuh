@@ -78,6 +78,13 @@ struct LsArgs {
     FftAxis ax[3];         // per axis (x, y, z)
 };
 
+// A pass plan: rows per row chunk, columns per strided tile, and the FFT
+// path (0 warp-owned lines where the axis allows it, 1 CTA-wide lines);
+// 0 / -1 fields ask for the defaults.
+struct LsPlan {
+    int rpb = 0, tk = 0, path = -1;
+};
+
 class BatchEngine;
 
 class LsSolver {
@@ -134,6 +141,18 @@ public:
     double asym(int k) const { return w_[k]; }
     cudaStream_t stream() const { return stream_; }
     int grid() const { return grid_; }
+    // Pass plan of the solver's launches, and the measured choice of one for
+    // `ncta` CTAs within smem_cap bytes of shared memory: every candidate
+    // (both FFT paths, row chunks of 1x/2x/4x the one-chunk-per-CTA size,
+    // column tiles of 1x/2x the default width) runs three LS iterations of the
+    // one-solve kernel on this solver's grid and moduli, on scratch copies of
+    // the state, and the fastest wins.  Choices are cached per device, grid
+    // shape and CTA count for the life of the process, so that solvers of
+    // one shape run one plan (and round alike).  MGK_LS_AUTOTUNE=0 in the
+    // environment turns the measurement off (the planner's defaults then).
+    const LsPlan& plan() const { return plan_; }
+    LsPlan tune(int ncta, size_t smem_cap);
+    static bool autotune_enabled();
     size_t device_bytes() const { return bytes_; }
 
 private:
@@ -156,6 +175,9 @@ private:
     unsigned* d_bar_ = nullptr;  // {arrivals, generation, err}
     std::vector<void*> tw_bufs_;
     LsArgs args_{};
+    void set_plan(const LsPlan& p);
+    LsPlan plan_;
+    int nsm_ = 148;
     int grid_ = 1, threads_ = 256;
     size_t smem_ = 0, bytes_ = 0;
 };
@@ -168,12 +190,14 @@ bool plan_radices(int n, FftAxis* ax);
 
 // Pass tiling of one solve run by ncta CTAs whose dynamic shared memory may
 // not exceed smem_cap bytes: rows per row chunk (rpb) and columns per strided
-// tile (tk) spread the work over the CTAs (a 0 argument picks them; given
-// values are clamped to what fits), and the shared-memory layout (line
-// buffer, second buffer for axes longer than kWarpFftMax, twiddle table).
-// Needs a.D, a.S, a.dims, a.N, a.nr, a.nh, a.nrows and the axes' radices.
-// Returns the dynamic shared-memory bytes of a launch, 0 when nothing fits.
-size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, int rpb = 0, int tk = 0);
+// tile (tk) spread the work over the CTAs (defaults: one chunk and one tile
+// per CTA, at least two rows a chunk in 2D; given values are clamped to what
+// fits), the FFT path of every axis (default: CTA-wide lines in 2D,
+// warp-owned lines in 3D, the faster of the two on B200 at these sizes), and
+// the shared-memory layout (two line buffers and the twiddle table).  Needs
+// a.D, a.S, a.dims, a.N, a.nr, a.nh, a.nrows and the axes' radices.  Returns
+// the dynamic shared-memory bytes of a launch, 0 when nothing fits.
+size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, LsPlan plan = LsPlan());
 // Work items of a plan: the larger of the row chunks and the column tiles
 // (a CTA beyond it idles in every pass).
 int plan_items(const LsArgs& a);
