@@ -74,6 +74,11 @@ MGK_API mgk_status mgk_ls_set_precision(mgk_ls* h, int precision);
 /* Device time (ms, CUDA events on the solver's stream) of the last solve's
  * kernel launches, without its host copies. */
 MGK_API mgk_status mgk_ls_last_solve_ms(mgk_ls* h, double* ms);
+/* No counterpart in the reference.  The pass plan the handle's solves run
+ * (chosen by timing candidates when the handle was created, unless the
+ * environment sets MGK_LS_AUTOTUNE=0): out4 = {rows per row chunk, columns
+ * per strided tile, FFT path (0 warp-owned lines, 1 CTA-wide lines), CTAs}. */
+MGK_API mgk_status mgk_ls_plan(mgk_ls* h, int* out4);
 /* No counterpart in the reference (which has no device waits).  Every
  * barrier wait inside the solver's persistent launch is bounded by device
  * time; this sets the bound (seconds; 0 restores the 120 s default).  A wait

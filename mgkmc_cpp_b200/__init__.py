@@ -78,6 +78,13 @@ class LsSolver:
             raise ValueError("precision must be 'fp64' or 'fp32_refined'")
         _lib.check(L.mgk_ls_set_precision(h, 1 if precision == "fp32_refined" else 0))
 
+    def plan(self) -> dict:
+        """The pass plan of this solver's launches (measured at creation)."""
+        out = (_lib.C.c_int * 4)()
+        _lib.check(_lib.lib().mgk_ls_plan(self._h, out))
+        return {"rows_per_chunk": out[0], "cols_per_tile": out[1], "fft": "warp" if out[2] == 0 else "cta",
+                "ctas": out[3]}
+
     def set_wait_limit(self, seconds: float):
         """Bound of every device-side barrier wait of the solver (0: 120 s)."""
         _lib.check(_lib.lib().mgk_ls_set_wait_limit(self._h, float(seconds)))

@@ -99,6 +99,16 @@ mgk_status mgk_ls_inject_absent_cta(mgk_ls* h, int cta) {
     return MGK_OK;
 }
 
+mgk_status mgk_ls_plan(mgk_ls* h, int* out4) {
+    if (!h || !out4) return fail(MGK_BAD_ARG, "null argument");
+    const mgk::LsPlan& p = h->solver->plan();
+    out4[0] = p.rpb;
+    out4[1] = p.tk;
+    out4[2] = p.path;
+    out4[3] = h->solver->grid();
+    return MGK_OK;
+}
+
 mgk_status mgk_ls_last_solve_ms(mgk_ls* h, double* ms) {
     if (!h || !ms) return fail(MGK_BAD_ARG, "null argument");
     *ms = h->solver->last_solve_ms();
