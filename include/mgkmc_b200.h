@@ -145,6 +145,17 @@ typedef struct {
                                                         a full LS solve every sync_interval flips (plain form only) */
     double ls_tol;            /* elastic_run tolerance, reference 1e-6 (:337) */
     int ls_max_iter;          /* reference 200 */
+    /* Extensions with no counterpart in the reference (0, 0: the reference's
+     * behaviour).  catalog_type: 0 the reference's random modes; 1 M shears in
+     * the x-y plane with slip directions evenly spaced in [0, pi) (magnitude
+     * gamma0, never redrawn); 2 (3D only) M plane normals on a Fibonacci
+     * lattice of the upper hemisphere, each sheared by gamma0 along its
+     * largest resolved shear stress, recomputed from the local stress where it
+     * is used (no per-mode catalog is stored).  barrier_per_voxel: one barrier
+     * per voxel shared by its M modes (drawn before the voxel's modes; redrawn
+     * as one value after a flip). */
+    int catalog_type;
+    int barrier_per_voxel;
 } mgk_kmc_params;
 
 /* run_simulation arguments (kmc_solver.hpp:721-729) plus a thermal-event cap. */

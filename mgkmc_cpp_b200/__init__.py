@@ -579,6 +579,8 @@ def kmc_params_from_config(cfg) -> "_lib.KmcParamsC":
     p.use_3d_barriers = int(bool(cfg.use_3d_barriers))
     p.fast_patching, p.patch_radius, p.sync_interval = int(bool(cfg.fast_patching)), cfg.patch_radius, cfg.sync_interval
     p.ls_tol, p.ls_max_iter = float(cfg.ls_tol), int(cfg.ls_max_iter)
+    p.catalog_type = {"random": 0, "even": 1, "fibonacci": 2}[cfg.catalog_type]
+    p.barrier_per_voxel = int(cfg.barrier_per_voxel)
     return p
 
 

@@ -8,7 +8,17 @@ including the GPa -> Pa auto-conversion (main.cpp:61-64, 96-99, 349-351) and the
 driving-component / mixed-target parsing (main.cpp:319-375).  Keys the reference
 never reads are ignored, as there.  New keys of this build live under new names
 (``ls.tol``, ``ls.max_iter``, ``run.max_flips``) and default to the reference's
-hard-coded values.
+hard-coded values.  Two keys select extensions with no counterpart in the
+reference (defaults: the reference's behaviour):
+
+* ``catalog.type``: ``random`` (the reference's modes, kmc_solver.hpp:231-238,
+  :1042-1074), ``even`` (M shears in the x-y plane with slip directions evenly
+  spaced in [0, pi), magnitude gamma0, never redrawn) or ``fibonacci`` (3D: M
+  plane normals on a Fibonacci lattice of the upper hemisphere, each sheared
+  by gamma0 along its largest resolved shear stress, recomputed from the
+  local stress whenever it is used);
+* ``barriers.per_voxel``: one barrier per voxel shared by its M modes (drawn
+  before the voxel's modes, and redrawn as one value after a flip).
 """
 from __future__ import annotations
 
@@ -207,6 +217,8 @@ class SimConfig:
     ls_tol: float = 1e-6
     ls_max_iter: int = 200
     max_flips: int = -1
+    catalog_type: str = "random"
+    barrier_per_voxel: bool = False
     output_directory: str = "simulation_results"
     summary_filename: str = "summary_log.txt"
     enable_console: bool = True
@@ -295,6 +307,12 @@ class SimConfig:
         s.ls_tol = c.get_double("ls.tol", 1e-6)
         s.ls_max_iter = c.get_int("ls.max_iter", 200)
         s.max_flips = c.get_int("run.max_flips", -1)
+        s.catalog_type = c.get_string("catalog.type", "random").lower()
+        if s.catalog_type not in ("random", "even", "fibonacci"):
+            raise ValueError("catalog.type must be random, even or fibonacci")
+        if s.catalog_type == "fibonacci" and s.dim != 3:
+            raise ValueError("catalog.type fibonacci needs a 3D system")
+        s.barrier_per_voxel = c.get_bool("barriers.per_voxel", False)
         return s
 
 

@@ -64,6 +64,7 @@ struct BatchRep {
     rng::Barrier bg;
     double gamma0;
     int redraw_dir, redraw_bar, C, pad0;
+    int ext, rd_dir, rd_bar, pad1;  // catalog / per-voxel barrier extensions and their RD_* redraw modes
     int ncta;
     unsigned* bar;  // {arrivals, generation, error, spare}
     dd* chunk_sum;
@@ -220,6 +221,25 @@ constexpr unsigned kAltBranch = 1u << 30;
 template <int C>
 MGK_DEV void redraw_seq(BatchRep& R, rng::Mt* g, long k) {
     const long v = k / R.s.M;
+    if (R.ext) {
+        // extensions (same order as the host-side draws of the plain form):
+        // the per-voxel barrier first, then the modes' draws; fixed catalogs
+        // draw no directions
+        const int M = R.s.M;
+        if (R.rd_bar == RD_VOXEL) {
+            const double q = rng::barrier(R.bg, g);
+            for (int mm = 0; mm < M; ++mm) R.s.Q0[v * M + mm] = q;
+        }
+        if (R.rd_dir == RD_ALL)
+            for (int mm = 0; mm < M; ++mm) rng::mode<C>(g, R.gamma0, R.s.cat + (v * M + mm) * C);
+        else if (R.rd_dir == RD_FLIPPED)
+            rng::mode<C>(g, R.gamma0, R.s.cat + k * C);
+        if (R.rd_bar == RD_ALL)
+            for (int mm = 0; mm < M; ++mm) R.s.Q0[v * M + mm] = rng::barrier(R.bg, g);
+        else if (R.rd_bar == RD_FLIPPED)
+            R.s.Q0[k] = rng::barrier(R.bg, g);
+        return;
+    }
     if (R.redraw_dir || R.redraw_bar) {
         for (int mm = 0; mm < R.s.M; ++mm) {
             const long ci = v * R.s.M + mm;
@@ -327,6 +347,15 @@ MGK_DEV void redraw_par(BatchRep& R, rng::MtRing* ring, rng::Mt* g, const int* m
     const bool need_r = us.do_bar && (us.btype == 2 || us.btype == 3);
     const rng::RayleighK rk = need_r ? rng::rayleigh_k(R.bg) : rng::RayleighK{0, 0, 0, 0};
     rng::ring_store(ring, g);  // starting state, for the fallback
+    if (R.ext) {
+        // the extensions' redraws are short (a per-voxel barrier, or the
+        // barriers of a fixed catalog): one thread walks them in order
+        if (threadIdx.x == 0)
+            for (int f = 0; f < nflips; ++f) redraw_seq<C>(R, g, modes[f]);
+        __syncthreads();
+        rng::ring_load(ring, g);
+        return;
+    }
     if (threadIdx.x == 0) {
         s_unit = 0;
         s_fail = 0;
@@ -1074,6 +1103,9 @@ void BatchEngine::init() {
         R.gamma0 = e.p_.gamma0;
         R.redraw_dir = e.p_.redraw_directions;
         R.redraw_bar = e.p_.redraw_barriers;
+        R.ext = e.p_.catalog_type != 0 || e.p_.barrier_per_voxel;
+        R.rd_dir = e.rd_dir_;
+        R.rd_bar = e.rd_bar_;
         R.C = e.C_;
         R.ncta = ncta_[r];
         auto alloc = [&](void** p, size_t b) {

@@ -84,9 +84,13 @@ KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu)
     if (p.nx < 1 || p.ny < 1 || (p.dim == 3 && p.nz < 1) || p.M < 1) throw std::invalid_argument("bad grid or M");
     if (p.fast_patching && (p.patch_radius < 0 || p.sync_interval < 1))
         throw std::invalid_argument("fast patching needs patch_radius >= 0 and sync_interval >= 1");
+    if (p.catalog_type < 0 || p.catalog_type > 2) throw std::invalid_argument("catalog_type must be 0, 1 or 2");
+    if (p.catalog_type == 2 && p.dim != 3) throw std::invalid_argument("the fibonacci catalog needs a 3D system");
+    if (p.catalog_type == 2 && p.fast_patching)
+        throw std::domain_error("fast patching needs a stored catalog (not the fibonacci catalog)");
     D_ = p.dim;
     S_ = D_ == 2 ? 3 : 6;
-    C_ = (D_ == 3 && p.use_3d_barriers) ? 6 : 2;
+    C_ = (D_ == 3 && (p.use_3d_barriers || p.catalog_type == 2)) ? 6 : 2;
     M_ = p.M;
     const long N = (long)p.nx * p.ny * (D_ == 3 ? p.nz : 1);
     if (N * (long)M_ > 0x7fffffffL) throw std::invalid_argument("N*M exceeds 2^31");
@@ -122,12 +126,40 @@ KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu)
     phys_.nx = p.nx;
     phys_.ny = p.ny;
     phys_.nz = D_ == 3 ? p.nz : 1;
-    // initial barriers and catalog, voxel-major / mode-minor (kmc_solver.hpp:222-240 / :1200-1215)
-    std::vector<double> Q0(NM_), cat(NM_ * C_);
+    // redraw modes of a flip (kmc_solver.hpp:839-864; the catalog and
+    // per-voxel barrier extensions: fixed catalogs are never redrawn, a
+    // per-voxel barrier is one value for all M modes)
+    {
+        const bool all = p.redraw_directions || p.redraw_barriers;
+        if (p.catalog_type == 0 && !p.barrier_per_voxel) {
+            rd_dir_ = all ? (p.redraw_directions ? RD_ALL : RD_NONE) : RD_FLIPPED;
+            rd_bar_ = all ? (p.redraw_barriers ? RD_ALL : RD_NONE) : RD_FLIPPED;
+        } else {
+            rd_dir_ = p.catalog_type != 0 ? RD_NONE : (p.redraw_directions ? RD_ALL : (all ? RD_NONE : RD_FLIPPED));
+            if (p.barrier_per_voxel) rd_bar_ = (p.redraw_barriers || !all) ? RD_VOXEL : RD_NONE;
+            else rd_bar_ = all ? (p.redraw_barriers ? RD_ALL : RD_NONE) : RD_FLIPPED;
+        }
+        nrec_ = (rd_dir_ == RD_ALL || rd_bar_ == RD_ALL) ? M_ : 1;
+    }
+    // initial barriers and catalog, voxel-major / mode-minor (kmc_solver.hpp:222-240 / :1200-1215);
+    // a per-voxel barrier is drawn before the voxel's modes
+    std::vector<double> Q0(NM_), cat(p.catalog_type == 2 ? 0 : NM_ * C_);
     std::normal_distribution<double> sn(0.0, 1.0);  // 2D: one object for the whole fill
-    for (long i = 0; i < NM_; ++i) {
-        Q0[i] = bar_.generate(rng_);
-        draw_mode(sn, &cat[i * C_]);
+    for (long v = 0; v < N; ++v) {
+        const double qv = p.barrier_per_voxel ? bar_.generate(rng_) : 0.0;
+        for (int m = 0; m < M_; ++m) {
+            const long i = v * M_ + m;
+            Q0[i] = p.barrier_per_voxel ? qv : bar_.generate(rng_);
+            if (p.catalog_type == 0) {
+                draw_mode(sn, &cat[i * C_]);
+            } else if (p.catalog_type == 1) {
+                // slip along (cos t, sin t) on the plane of normal (-sin t, cos t),
+                // t = m pi / M: (gamma0/2) [[-sin 2t, cos 2t], [cos 2t, sin 2t]]
+                const double a = 2.0 * M_PI * (double)m / (double)M_;
+                cat[i * C_] = -0.5 * p.gamma0 * std::sin(a);
+                cat[i * C_ + 1] = 0.5 * p.gamma0 * std::cos(a);
+            }
+        }
     }
     // device state
     auto alloc = [&](void** ptr, size_t b) { CK(cudaMalloc(ptr, b)); };
@@ -139,7 +171,28 @@ KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu)
     dev_.NM = NM_;
     alloc((void**)&dev_.Q0, sizeof(double) * NM_);
     alloc((void**)&dev_.Q, sizeof(double) * NM_);
-    alloc((void**)&dev_.cat, sizeof(double) * NM_ * C_);
+    dev_.cat = nullptr;
+    dev_.normals = nullptr;
+    dev_.gamma0 = p.gamma0;
+    if (p.catalog_type == 2) {
+        // Fibonacci lattice on the upper hemisphere: z = 1 - (m + 1/2) / M,
+        // azimuth m pi (3 - sqrt 5)
+        std::vector<double> nv(3 * (size_t)M_);
+        const double ga = M_PI * (3.0 - std::sqrt(5.0));
+        for (int m = 0; m < M_; ++m) {
+            const double z = 1.0 - ((double)m + 0.5) / (double)M_;
+            const double r = std::sqrt(1.0 - z * z);
+            const double ph = (double)m * ga;
+            nv[3 * m] = r * std::cos(ph);
+            nv[3 * m + 1] = r * std::sin(ph);
+            nv[3 * m + 2] = z;
+        }
+        alloc((void**)&d_normals_, sizeof(double) * 3 * M_);
+        CK(cudaMemcpy(d_normals_, nv.data(), sizeof(double) * 3 * M_, cudaMemcpyHostToDevice));
+        dev_.normals = d_normals_;
+    } else {
+        alloc((void**)&dev_.cat, sizeof(double) * NM_ * C_);
+    }
     alloc((void**)&dev_.epsp_s, sizeof(double) * S_ * N);
     alloc((void**)&dev_.soft, sizeof(double) * 2 * N);
     alloc((void**)&dev_.last_t, sizeof(double) * N);
@@ -148,7 +201,7 @@ KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu)
     dev_.lam = ls_->lam();
     dev_.mu = ls_->mu();
     CK(cudaMemcpy(dev_.Q0, Q0.data(), sizeof(double) * NM_, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(dev_.cat, cat.data(), sizeof(double) * NM_ * C_, cudaMemcpyHostToDevice));
+    if (dev_.cat) CK(cudaMemcpy(dev_.cat, cat.data(), sizeof(double) * NM_ * C_, cudaMemcpyHostToDevice));
     CK(cudaMemset(dev_.Q, 0, sizeof(double) * NM_));
     CK(cudaMemset(dev_.epsp_s, 0, sizeof(double) * S_ * N));
     CK(cudaMemset(dev_.soft, 0, sizeof(double) * 2 * N));
@@ -292,6 +345,7 @@ KmcEngine::~KmcEngine() {
     cudaFree(dev_.Q0);
     cudaFree(dev_.Q);
     cudaFree(dev_.cat);
+    cudaFree(d_normals_);
     cudaFree(dev_.epsp_s);
     cudaFree(dev_.soft);
     cudaFree(dev_.last_t);
@@ -371,9 +425,23 @@ void KmcEngine::draw_mode(std::normal_distribution<double>& sn, double* out) {
     out[5] = G[1][2] * mag;
 }
 
-// One flip's redraw values (kmc_solver.hpp:839-864 / :1854-1875), in draw order.
+// One flip's redraw values (kmc_solver.hpp:839-864 / :1854-1875), in draw
+// order, as nrec_ records of C + 1 values for the rd_dir_ / rd_bar_ modes.
 void KmcEngine::gen_flip_draws(double* out) {
     std::normal_distribution<double> sn(0.0, 1.0);
+    if (p_.catalog_type != 0 || p_.barrier_per_voxel) {
+        // extensions: the per-voxel barrier first, then the modes' draws
+        if (rd_bar_ == RD_VOXEL) out[C_] = bar_.generate(rng_);
+        if (rd_dir_ == RD_ALL)
+            for (int mm = 0; mm < M_; ++mm) draw_mode(sn, out + (size_t)mm * (C_ + 1));
+        else if (rd_dir_ == RD_FLIPPED)
+            draw_mode(sn, out);
+        if (rd_bar_ == RD_ALL)
+            for (int mm = 0; mm < M_; ++mm) out[(size_t)mm * (C_ + 1) + C_] = bar_.generate(rng_);
+        else if (rd_bar_ == RD_FLIPPED)
+            out[C_] = bar_.generate(rng_);
+        return;
+    }
     if (p_.redraw_directions || p_.redraw_barriers) {
         for (int mm = 0; mm < M_; ++mm) {
             double* r = out + (size_t)mm * (C_ + 1);
@@ -505,7 +573,7 @@ mgk_status KmcEngine::elastic_run() {
 mgk_status KmcEngine::run_cascade(int* steps, int* flips, long long cap) {
     int total = 0, local = 0;
     const long long limit = cap > 0 ? cap : (long long)N_;
-    const size_t rec = (size_t)((p_.redraw_directions || p_.redraw_barriers) ? M_ : 1) * (C_ + 1);
+    const size_t rec = (size_t)nrec_ * (C_ + 1);
     while (true) {
         if (h_status_->n_unstable == 0) break;
         int zero = 0;
@@ -529,8 +597,8 @@ mgk_status KmcEngine::run_cascade(int* steps, int* flips, long long cap) {
         }
         for (int f = 0; f < n; ++f) gen_flip_draws(h_upload_ + (size_t)f * rec);
         CK(cudaMemcpyAsync(d_upload_, h_upload_, sizeof(double) * need, cudaMemcpyHostToDevice, st_));
-        CK(kmc_cascade_flip(dev_, phys_, d_ckeys_, d_cmodes_, n, d_ckeys2_, d_cmodes2_, time_, d_upload_,
-                            p_.redraw_directions, p_.redraw_barriers, d_status_, st_));
+        CK(kmc_cascade_flip(dev_, phys_, d_ckeys_, d_cmodes_, n, d_ckeys2_, d_cmodes2_, time_, d_upload_, rd_dir_,
+                            rd_bar_, d_status_, st_));
         {
             int np2 = 1, lg = 0;
             while (np2 < n) np2 <<= 1;
@@ -749,12 +817,12 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
                         remaining -= tw;
                         h_upload_[0] = U(rng_) * R;
                         gen_flip_draws(h_upload_ + 1);
-                        const size_t nup = 1 + (size_t)((p_.redraw_directions || p_.redraw_barriers) ? M_ : 1) * (C_ + 1);
+                        const size_t nup = 1 + (size_t)nrec_ * (C_ + 1);
                         CK(cudaMemcpyAsync(d_upload_, h_upload_, sizeof(double) * nup, cudaMemcpyHostToDevice, st_));
                         prof_begin(2);
                         stats_.launches += 1;
                         CK(kmc_select_flip(dev_, phys_, d_blk_, d_blk_last_, nblk_, items_, d_upload_, time_, d_upload_ + 1,
-                                           p_.redraw_directions, p_.redraw_barriers, d_status_, st_));
+                                           rd_dir_, rd_bar_, d_status_, st_));
                         prof_end(2);
                         if (fp_) {  // kmc_solver.hpp:866-915: predictor, stencil, LS only every sync_interval flips
                             s = patch_after_flips(&d_status_->selected, 1, tw > 0.0 ? p_.strain_rate * tw : 0.0, true,
@@ -898,7 +966,7 @@ mgk_status KmcEngine::get_field(int field, double* dst, long long* count) {
         case 3: n = 2 * N; break;
         case 4: case 9: case 10: n = N; break;
         case 5: case 6: n = NM_; break;
-        case 7: n = NM_ * DD; break;
+        case 7: n = dev_.cat ? NM_ * DD : 0; break;  // stress-dependent modes: no stored catalog
         default: last_error = "unknown field"; return MGK_BAD_ARG;
     }
     if (count) *count = n;
@@ -963,6 +1031,7 @@ mgk_status KmcEngine::get_field(int field, double* dst, long long* count) {
         } else if (field == 6) {
             CK(cudaMemcpy(dst, dev_.Q0, sizeof(double) * NM_, cudaMemcpyDeviceToHost));
         } else if (field == 7) {
+            if (!dev_.cat) return MGK_OK;
             std::vector<double> c((size_t)NM_ * C_);
             CK(cudaMemcpy(c.data(), dev_.cat, sizeof(double) * NM_ * C_, cudaMemcpyDeviceToHost));
             for (long i = 0; i < NM_; ++i) cat_full(&c[(size_t)i * C_], dst + i * DD);

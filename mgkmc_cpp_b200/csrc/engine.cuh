@@ -84,6 +84,8 @@ private:
 
     mgk_kmc_params p_;
     int D_, S_, C_, M_, N_;
+    int rd_dir_ = 0, rd_bar_ = 0, nrec_ = 1;  // RD_* redraw modes of a flip, records per flip
+    double* d_normals_ = nullptr;             // catalog_type 2: M plane normals
     long NM_;
     cudaStream_t st_ = nullptr;
     std::unique_ptr<LsSolver> ls_;

@@ -52,18 +52,82 @@ MGK_DEV int voxel_of(long i, long NM, int M) {
     return NM <= 0xffffffffL ? (int)((unsigned)i / (unsigned)M) : (int)(i / M);
 }
 
+// Shear of magnitude gamma0 on the plane of normal n along the largest
+// resolved shear traction tau = sigma n - (n . sigma n) n (where tau vanishes,
+// along the projection of x -- or y when n is near x -- onto the plane);
+// symmetric components of (gamma0 / 2)(s n + n s).  sg: symmetric stress
+// {xx, yy, zz, xy, xz, yz}.  The catalog extension "fibonacci" (no
+// counterpart in the reference).
+MGK_DEV void fib_mode(const double* sg, const double* n, double gamma0, double* o) {
+    const double sf[9] = {sg[0], sg[3], sg[4], sg[3], sg[1], sg[5], sg[4], sg[5], sg[2]};
+    double t[3], tau[3], sv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) t[i] = sf[3 * i] * n[0] + sf[3 * i + 1] * n[1] + sf[3 * i + 2] * n[2];
+    const double tn = t[0] * n[0] + t[1] * n[1] + t[2] * n[2];
+    double tt = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        tau[i] = t[i] - tn * n[i];
+        tt += tau[i] * tau[i];
+    }
+    if (tt > 0.0) {
+        const double inv = 1.0 / sqrt(tt);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) sv[i] = tau[i] * inv;
+    } else {
+        double e[3] = {0.0, 0.0, 0.0};
+        e[fabs(n[0]) < 0.9 ? 0 : 1] = 1.0;
+        const double d = e[0] * n[0] + e[1] * n[1] + e[2] * n[2];
+        double q = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            sv[i] = e[i] - d * n[i];
+            q += sv[i] * sv[i];
+        }
+        const double inv = 1.0 / sqrt(q);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) sv[i] *= inv;
+    }
+    const double h = 0.5 * gamma0;
+    o[0] = h * (sv[0] * n[0] + n[0] * sv[0]);
+    o[1] = h * (sv[1] * n[1] + n[1] * sv[1]);
+    o[2] = h * (sv[2] * n[2] + n[2] * sv[2]);
+    o[3] = h * (sv[0] * n[1] + n[0] * sv[1]);
+    o[4] = h * (sv[0] * n[2] + n[0] * sv[2]);
+    o[5] = h * (sv[1] * n[2] + n[1] * sv[2]);
+}
+
+// Symmetric components of mode i (of voxel v, stress sg) now: the catalog
+// entry, or the stress-dependent shear of the mode's plane.
+template <int D, int C>
+MGK_DEV void mode_eps(const KmcDevState& s, int v, long i, const double* sg, double* cs) {
+    if (D == 3 && s.normals) {
+        const int m = (int)(i - (long)v * s.M);
+        fib_mode(sg, s.normals + 3 * m, s.gamma0, cs);
+    } else {
+        cat_sym<D, C>(s.cat + i * C, cs);
+    }
+}
+
+// Stress of voxel v as the sweep reads it (the kept field with fast patching)
+template <int D>
+MGK_DEV void sweep_stress(const KmcDevState& s, int v, double* sg) {
+    constexpr int S = D == 2 ? 3 : 6;
+    if (s.sig_s) {
+#pragma unroll
+        for (int c = 0; c < S; ++c) sg[c] = s.sig_s[(long)c * s.N + v];
+    } else {
+        voxel_stress<D>(s, v, sg);
+    }
+}
+
 // Q of mode i at voxel v (update_barriers, kmc_solver.hpp:345-407 / :1344-1406)
 template <int D, int C>
 MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, double time) {
     constexpr int S = D == 2 ? 3 : 6;
     const int N = s.N;
     double sg[S];
-    if (s.sig_s) {  // fast patching: the kept stress field
-#pragma unroll
-        for (int c = 0; c < S; ++c) sg[c] = s.sig_s[(long)c * N + v];
-    } else {
-        voxel_stress<D>(s, v, sg);
-    }
+    sweep_stress<D>(s, v, sg);
     // softening state
     const double gt = s.soft[2 * v + 1];
     double gtc = 0.0;
@@ -79,9 +143,8 @@ MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, dou
     }
     double gb = s.soft[2 * v] + gtc;
     if (p.softening_cap > 0.0 && gb > p.softening_cap) gb = p.softening_cap;
-    const double* cm = s.cat + i * C;
     double cs[S];
-    cat_sym<D, C>(cm, cs);
+    mode_eps<D, C>(s, v, i, sg, cs);
     double mod = 1.0;
     if (p.directional) {
         double ps[S];
@@ -162,8 +225,14 @@ MGK_DEV void apply_flip(const KmcDevState& s, const KmcPhys& p, long k, double t
     constexpr int S = D == 2 ? 3 : 6;
     const int v = (int)(k / s.M);
     double c[6];
+    if (D == 3 && s.normals) {  // stress-dependent mode: C = 6 symmetric components
+        double sg[6];
+        sweep_stress<D>(s, v, sg);
+        mode_eps<D, C>(s, v, k, sg, c);
+    } else {
 #pragma unroll
-    for (int j = 0; j < C; ++j) c[j] = s.cat[k * C + j];
+        for (int j = 0; j < C; ++j) c[j] = s.cat[k * C + j];
+    }
     double cs[S];
     cat_sym<D, C>(c, cs);
 #pragma unroll
@@ -205,20 +274,22 @@ MGK_DEV void apply_flip(const KmcDevState& s, const KmcPhys& p, long k, double t
 
 template <int C>
 MGK_DEV void redraw(const KmcDevState& s, long k, const double* draws, int redraw_dir, int redraw_bar, int tid, int nthr) {
-    // kmc_solver.hpp:841-864: all M modes of the voxel when either flag is set,
-    // else only the flipped mode; draws hold M (or 1) records of C + 1 values.
+    // kmc_solver.hpp:841-864 and the per-voxel barrier extension: the RD_*
+    // modes of the two parts; draws hold M records of C + 1 values when either
+    // part is RD_ALL, else one record.
     const long v = k / s.M;
-    if (redraw_dir || redraw_bar) {
-        for (int mm = tid; mm < s.M; mm += nthr) {
-            const long ci = v * s.M + mm;
-            const double* d = draws + (long)mm * (C + 1);
-            if (redraw_dir)
-                for (int j = 0; j < C; ++j) s.cat[ci * C + j] = d[j];
-            if (redraw_bar) s.Q0[ci] = d[C];
-        }
-    } else if (tid == 0) {
-        for (int j = 0; j < C; ++j) s.cat[k * C + j] = draws[j];
-        s.Q0[k] = draws[C];
+    for (int mm = tid; mm < s.M; mm += nthr) {
+        const long ci = v * s.M + mm;
+        const double* d = draws + (long)mm * (C + 1);
+        if (redraw_dir == RD_ALL)
+            for (int j = 0; j < C; ++j) s.cat[ci * C + j] = d[j];
+        if (redraw_bar == RD_ALL) s.Q0[ci] = d[C];
+        if (redraw_bar == RD_VOXEL) s.Q0[ci] = draws[C];
+    }
+    if (tid == 0) {
+        if (redraw_dir == RD_FLIPPED)
+            for (int j = 0; j < C; ++j) s.cat[k * C + j] = draws[j];
+        if (redraw_bar == RD_FLIPPED) s.Q0[k] = draws[C];
     }
 }
 

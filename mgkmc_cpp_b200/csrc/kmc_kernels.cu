@@ -309,7 +309,7 @@ __global__ void pad_kernel(const double* keys, const int* modes, int n, int npow
 template <int D, int C>
 __global__ void cascade_apply_kernel(KmcDevState s, KmcPhys p, const int* modes, int n, double time, const double* draws,
                                      int redraw_dir, int redraw_bar) {
-    const int rec = (redraw_dir || redraw_bar) ? s.M : 1;
+    const int rec = (redraw_dir == RD_ALL || redraw_bar == RD_ALL) ? s.M : 1;
     if (p.neigh > 0.0) {
         if (blockIdx.x != 0) return;
         for (int f = 0; f < n; ++f) {

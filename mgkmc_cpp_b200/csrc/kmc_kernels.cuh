@@ -28,7 +28,22 @@ struct KmcDevState {
     // select / cascade batch, the flipped mode's catalog entry before its redraw
     double* sig_s;        // S * N
     double* flipcat;      // N * C
+    // stress-dependent catalog (catalog.type fibonacci; else null): M plane
+    // normals (x, y, z); every mode is a shear of magnitude gamma0 along the
+    // plane's largest resolved shear stress, computed where it is used; cat is
+    // then null and prev / flipcat hold C = 6 symmetric components
+    const double* normals;
+    double gamma0;
 };
+
+// How a flip's redraw records (kmc_select_flip, kmc_cascade_flip) replace the
+// voxel's modes.  Directions: none, all M modes from M records, or the
+// flipped mode from record 0.  Barriers: none, all M from M records, the
+// flipped mode from record 0, or one value (record 0) for all M modes (a
+// barrier per voxel).  The reference's redraw (kmc_solver.hpp:839-864) is
+// (ALL, ALL) with both flags set, (ALL, NONE) / (NONE, ALL) with one, and
+// (FLIPPED, FLIPPED) with neither.
+enum : int { RD_NONE = 0, RD_ALL = 1, RD_FLIPPED = 2, RD_VOXEL = 3 };
 
 struct KmcPhys {
     double volume;        // pixel^3 (work term)
@@ -61,9 +76,9 @@ cudaError_t kmc_sweep(const KmcDevState& s, const KmcPhys& p, double time, dd* b
                       int items, KmcStatus* status, cudaStream_t st);
 int kmc_sweep_blocks(long NM, int items);
 // Select the first mode whose rate prefix reaches `target` (from the host:
-// u2 * total) and apply the flip at simulation time `time` with the M redraw
-// records in `draws` (M x (C + 1): catalog values then Q0; `redraw_dir`,
-// `redraw_bar` say which parts are replaced).
+// u2 * total) and apply the flip at simulation time `time` with the redraw
+// records in `draws` (M or 1 records of C + 1 values: catalog values then Q0;
+// `redraw_dir`, `redraw_bar` are RD_* modes saying which parts replace what).
 cudaError_t kmc_select_flip(const KmcDevState& s, const KmcPhys& p, const dd* blk, const int* blk_last, int nblk, int items,
                             const double* target_dev, double time, const double* draws, int redraw_dir, int redraw_bar,
                             KmcStatus* status, cudaStream_t st);

@@ -65,8 +65,10 @@ material:
   nu:
     mode: "constant"
     value: 0.36
+catalog:
+  type: "{cat}"
 loading:
-  eps_target: 0.05
+  eps_target: {eps_target}
   step_size: 1e-4
 boundary_conditions:
   driving_component: "{drive}"
@@ -75,6 +77,7 @@ boundary_conditions:
   mixed_tol: 1.0
 barriers:
   type: "gaussian"
+  per_voxel: {pv}
   kwargs:
     mean: {bmean}
     std: {bstd}
@@ -115,6 +118,24 @@ for _n in (64, 128, 512):
 for _n in (32, 48, 96):
     WORKLOADS["ens3d_%d" % _n] = dict(dim="3d", nx=_n, ny=_n, nz=_n, M=100, b3="true", hetero=("draw", 3.0), **_T3,
                                       **_B_REF, gamma0=0.03)
+
+# The benchmark description's own physics, through the catalog and per-voxel
+# barrier extensions (catalog.type, barriers.per_voxel; no counterpart in the
+# reference, whose random catalog these replace):
+#   bl_cfg0_32   2D 32^2 homogeneous, 18 shears evenly spaced in [0, pi),
+#                dF = 1.0 eV in every voxel (per voxel, sd 0)
+#   bl_cfg1_256  2D 256^2 lognormal E (CoV 0.1, correlation 4), 18 even
+#                shears, dF per voxel N(1.0, 0.1) eV clipped to [0.6, 1.4]
+#   bl_cfg2_64   3D 64^3 lognormal E (CoV 0.15, correlation 3), 100 Fibonacci
+#                plane normals sheared along their largest resolved shear
+#                stress, gamma0 0.1, dF per voxel as above, z tension to 3 %
+_BL = dict(pv="true", **_B_DF1)
+WORKLOADS["bl_cfg0_32"] = dict(dim="2d", nx=32, ny=32, nz=1, M=18, b3="false", hetero=None, **_T2, cat="even",
+                               pv="true", bmean="1.0", bstd="0.0", bmin="0.6", bmax="1.4")
+WORKLOADS["bl_cfg1_256"] = dict(dim="2d", nx=256, ny=256, nz=1, M=18, b3="false", hetero=(0.10, 4.0), **_T2, cat="even",
+                                **_BL)
+WORKLOADS["bl_cfg2_64"] = dict(dim="3d", nx=64, ny=64, nz=64, M=100, b3="false", hetero=(0.15, 3.0), **_T3,
+                               cat="fibonacci", eps_target=0.03, **_BL)
 
 ENSEMBLE = ["ens2d_64"] * 16 + ["ens2d_128"] * 16 + ["ens2d_512"] * 16 + ["ens3d_32"] * 5 + ["ens3d_48"] * 5 + \
     ["ens3d_96"] * 6
@@ -174,6 +195,9 @@ def write_workload(name: str, directory: str, seed: int = 0) -> Tuple[str, SimCo
         eblock = '    mode: "file"\n    parameters:\n      path: "%s"' % epath
     fmt = {k: v for k, v in w.items() if k != "hetero"}
     fmt.setdefault("gamma0", 0.1)
+    fmt.setdefault("cat", "random")
+    fmt.setdefault("pv", "false")
+    fmt.setdefault("eps_target", 0.05)
     text = _BASE.format(seed=seed, Eblock=eblock, **fmt)
     path = os.path.join(directory, "%s_s%d.yaml" % (name, seed))
     with open(path, "w") as f:

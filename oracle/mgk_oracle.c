@@ -359,6 +359,12 @@ typedef struct {
     int n_targets;
     int target_i[9], target_j[9];
     double target_v[9];
+    /* catalog extensions (no counterpart in the reference): catalog_type 0
+     * the reference's random modes, 1 M shears evenly spaced in [0, pi) in the
+     * x-y plane, 2 (3D) M Fibonacci-lattice plane normals sheared along their
+     * largest resolved shear stress; barrier_per_voxel: one barrier per voxel
+     * shared by its M modes */
+    int catalog_type, barrier_per_voxel;
 } kmc_params;
 
 typedef struct {
@@ -367,6 +373,7 @@ typedef struct {
     int D, DD;
     double volume, tau, time;
     double *E, *nu, *eps, *sig, *epsp, *soft, *last_t, *Q, *Q0, *cat, *prev;
+    double* normals;  /* catalog_type 2: M plane normals (x, y, z) */
     double eps_macro[9], sig_macro[9];
     mt19937 rng;
     int ls_iters_total, ls_solves;
@@ -403,8 +410,78 @@ static void draw_mode(kmc_state* s, normal_state* ns, double* out) {
     out[0] = gxx; out[D + 1] = -gxx; out[1] = gxy; out[D] = gxy;
 }
 
+/* Catalog extensions (no counterpart in the reference).
+ * Even: shear m of M slips along s = (cos t, sin t, 0) on the plane of normal
+ * n = (-sin t, cos t, 0), t = m pi / M; eigenstrain (gamma0 / 2)(s n + n s):
+ * xx = -(gamma0/2) sin 2t, yy = +(gamma0/2) sin 2t, xy = (gamma0/2) cos 2t. */
+static void even_mode(const kmc_state* s, int m, double* out) {
+    const int D = s->D;
+    const double h = 0.5 * s->p.gamma0;
+    const double a = 2.0 * M_PI * (double)m / (double)s->p.M;
+    const double sa = sin(a), ca = cos(a);
+    memset(out, 0, sizeof(double) * s->DD);
+    out[0] = -h * sa;
+    out[D + 1] = h * sa;
+    out[1] = h * ca;
+    out[D] = h * ca;
+}
+
+/* Fibonacci lattice on the upper hemisphere: z = 1 - (m + 1/2) / M,
+ * azimuth m * pi (3 - sqrt 5). */
+static void fib_normals(int M, double* n) {
+    const double ga = M_PI * (3.0 - sqrt(5.0));
+    for (int m = 0; m < M; ++m) {
+        const double z = 1.0 - ((double)m + 0.5) / (double)M;
+        const double r = sqrt(1.0 - z * z);
+        const double ph = (double)m * ga;
+        n[3 * m] = r * cos(ph);
+        n[3 * m + 1] = r * sin(ph);
+        n[3 * m + 2] = z;
+    }
+}
+
+/* Stress-dependent shear on the plane of normal n: slip along the resolved
+ * shear traction tau = sigma n - (n . sigma n) n (where tau vanishes, along the
+ * projection of x -- or y when n is near x -- onto the plane); eigenstrain
+ * (gamma0 / 2)(s n + n s), so that sigma : eps0 = gamma0 |tau|. */
+static void fib_mode(const double* sg, const double* n, double gamma0, double* out) {
+    double t[3], tau[3], sv[3];
+    for (int i = 0; i < 3; ++i) t[i] = sg[3 * i] * n[0] + sg[3 * i + 1] * n[1] + sg[3 * i + 2] * n[2];
+    const double tn = t[0] * n[0] + t[1] * n[1] + t[2] * n[2];
+    double tt = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        tau[i] = t[i] - tn * n[i];
+        tt += tau[i] * tau[i];
+    }
+    if (tt > 0.0) {
+        const double inv = 1.0 / sqrt(tt);
+        for (int i = 0; i < 3; ++i) sv[i] = tau[i] * inv;
+    } else {
+        double e[3] = {0.0, 0.0, 0.0};
+        e[fabs(n[0]) < 0.9 ? 0 : 1] = 1.0;
+        const double d = e[0] * n[0] + e[1] * n[1] + e[2] * n[2];
+        double q = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            sv[i] = e[i] - d * n[i];
+            q += sv[i] * sv[i];
+        }
+        const double inv = 1.0 / sqrt(q);
+        for (int i = 0; i < 3; ++i) sv[i] *= inv;
+    }
+    const double h = 0.5 * gamma0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out[3 * i + j] = h * (sv[i] * n[j] + n[i] * sv[j]);
+}
+
+/* the eigenstrain of mode m of voxel v now (full D x D row-major) */
+static void mode_of(const kmc_state* s, long v, int m, double* out) {
+    if (s->p.catalog_type == 2) fib_mode(s->sig + v * 9, s->normals + 3 * m, s->p.gamma0, out);
+    else memcpy(out, s->cat + (v * s->p.M + m) * s->DD, sizeof(double) * s->DD);
+}
+
 /* constructors, kmc_solver.hpp:165-257 / 1142-1232 */
 void* oracle_kmc_create(const kmc_params* p, const double* E, const double* nu) {
+    if (p->catalog_type == 2 && p->dim != 3) return NULL;  /* plane normals need 3D */
     kmc_state* s = calloc(1, sizeof(kmc_state));
     s->p = *p;
     s->D = p->dim; s->DD = p->dim * p->dim;
@@ -421,18 +498,26 @@ void* oracle_kmc_create(const kmc_params* p, const double* E, const double* nu) 
     for (long i = 0; i < N; ++i) s->last_t[i] = -INFINITY;
     s->Q = calloc(NM, sizeof(double));
     s->Q0 = malloc(sizeof(double) * NM);
-    s->cat = calloc(NM * s->DD, sizeof(double));
+    s->cat = p->catalog_type == 2 ? NULL : calloc(NM * s->DD, sizeof(double));
+    if (p->catalog_type == 2) {
+        s->normals = malloc(sizeof(double) * 3 * p->M);
+        fib_normals(p->M, s->normals);
+    }
     s->prev = calloc(N * s->DD, sizeof(double));
     if (p->temperature > 0.0) s->tau = 1.0 / (p->nu0 * exp(-p->q_act_temp / (8.617e-5 * p->temperature)));
     else s->tau = INFINITY;
     mt_seed(&s->rng, (uint32_t)p->seed);
     normal_state ns = {0.0, 0};  /* 2D ctor: one normal object for the whole fill */
-    for (long v = 0; v < N; ++v)
+    for (long v = 0; v < N; ++v) {
+        /* extension: one barrier per voxel, drawn before the voxel's modes */
+        double qv = p->barrier_per_voxel ? oracle_barrier_draw(&p->bar, &s->rng) : 0.0;
         for (int m = 0; m < p->M; ++m) {
             long mi = v * p->M + m;
-            s->Q0[mi] = oracle_barrier_draw(&p->bar, &s->rng);
-            draw_mode(s, &ns, s->cat + mi * s->DD);
+            s->Q0[mi] = p->barrier_per_voxel ? qv : oracle_barrier_draw(&p->bar, &s->rng);
+            if (p->catalog_type == 0) draw_mode(s, &ns, s->cat + mi * s->DD);
+            else if (p->catalog_type == 1) even_mode(s, m, s->cat + mi * s->DD);
         }
+    }
     return s;
 }
 
@@ -440,7 +525,7 @@ void oracle_kmc_destroy(void* h) {
     kmc_state* s = h;
     if (!s) return;
     free(s->E); free(s->nu); free(s->eps); free(s->sig); free(s->epsp); free(s->soft); free(s->last_t);
-    free(s->Q); free(s->Q0); free(s->cat); free(s->prev); free(s);
+    free(s->Q); free(s->Q0); free(s->cat); free(s->prev); free(s->normals); free(s);
 }
 
 /* elastic_run, kmc_solver.hpp:334-339 / 1333-1338 */
@@ -471,7 +556,9 @@ static void update_barriers(kmc_state* s) {
         const double* pv = s->prev + v * DD;
         for (int m = 0; m < M; ++m) {
             long mi = v * M + m;
-            const double* c = s->cat + mi * DD;
+            double cm[9];
+            mode_of(s, v, m, cm);
+            const double* c = cm;
             double mod = 1.0;
             if (s->p.directional) {
                 double dp = 0.0, nm = 0.0, np = 0.0;
@@ -490,7 +577,9 @@ static void update_barriers(kmc_state* s) {
 /* apply_flip_soa_2d / _3d, kmc_solver.hpp:423-462 / 1424-1471 */
 static void apply_flip(kmc_state* s, long vox, int m) {
     const int D = s->D, DD = s->DD;
-    const double* c = s->cat + (vox * s->p.M + m) * DD;
+    double cm[9];
+    mode_of(s, vox, m, cm);
+    const double* c = cm;
     for (int k = 0; k < DD; ++k) s->epsp[vox * DD + k] += c[k];
     double ssq;
     if (D == 2) {
@@ -527,6 +616,26 @@ static void apply_flip(kmc_state* s, long vox, int m) {
 static void redraw(kmc_state* s, long vox, long flat) {
     normal_state ns = {0.0, 0};
     const int M = s->p.M, DD = s->DD;
+    if (s->p.catalog_type != 0 || s->p.barrier_per_voxel) {
+        /* extensions: fixed catalogs are never redrawn; a per-voxel barrier is
+         * one draw before the voxel's modes */
+        const int rd = s->p.redraw_directions && s->p.catalog_type == 0;
+        const int all = s->p.redraw_directions || s->p.redraw_barriers;
+        if (s->p.barrier_per_voxel) {
+            if (s->p.redraw_barriers || !all) {
+                const double q = oracle_barrier_draw(&s->p.bar, &s->rng);
+                for (int mm = 0; mm < M; ++mm) s->Q0[vox * M + mm] = q;
+            }
+            if (rd) for (int mm = 0; mm < M; ++mm) draw_mode(s, &ns, s->cat + (vox * M + mm) * DD);
+            else if (!all && s->p.catalog_type == 0) draw_mode(s, &ns, s->cat + flat * DD);
+        } else if (all) {
+            if (s->p.redraw_barriers)
+                for (int mm = 0; mm < M; ++mm) s->Q0[vox * M + mm] = oracle_barrier_draw(&s->p.bar, &s->rng);
+        } else {
+            s->Q0[flat] = oracle_barrier_draw(&s->p.bar, &s->rng);
+        }
+        return;
+    }
     if (s->p.redraw_directions || s->p.redraw_barriers) {
         for (int mm = 0; mm < M; ++mm) {
             long ci = vox * M + mm;
@@ -568,7 +677,7 @@ static void run_cascade(kmc_state* s, int* steps, int* flips) {
             if (seen[vox]) continue;
             seen[vox] = 1;
             ++nb;
-            memcpy(s->prev + vox * s->DD, s->cat + mi * s->DD, sizeof(double) * s->DD);
+            mode_of(s, vox, m, s->prev + vox * s->DD);
             apply_flip(s, vox, m);
             redraw(s, vox, mi);
         }
@@ -648,7 +757,7 @@ long oracle_kmc_run(void* h, int nsteps, long maxev, double* trace, long trace_c
                     long f = idx[sel], vox = f / s->p.M;
                     int m = (int)(f % s->p.M);
                     int instab = s->Q[f] <= s->p.stability_threshold;
-                    memcpy(s->prev + vox * DD, s->cat + f * DD, sizeof(double) * DD);
+                    mode_of(s, vox, m, s->prev + vox * DD);
                     apply_flip(s, vox, m);
                     redraw(s, vox, f);
                     elastic_run(s);
@@ -710,7 +819,7 @@ long oracle_kmc_get(void* h, int field, double* out) {
         case 4: src = s->last_t; n = s->N; break;
         case 5: src = s->Q; n = NM; break;
         case 6: src = s->Q0; n = NM; break;
-        case 7: src = s->cat; n = NM * s->DD; break;
+        case 7: src = s->cat; n = src ? NM * s->DD : 0; break;  /* stress-dependent modes: none stored */
         case 8: src = s->prev; n = s->N * s->DD; break;
         default: return -1;
     }

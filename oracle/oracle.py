@@ -70,7 +70,11 @@ class KmcParams(C.Structure):
                 ("redraw_directions", C.c_int), ("redraw_barriers", C.c_int), ("use_3d_barriers", C.c_int),
                 ("step_size", C.c_double), ("mixed_tol", C.c_double), ("max_kmc_steps_pct", C.c_double),
                 ("comp_i", C.c_int), ("comp_j", C.c_int), ("n_targets", C.c_int), ("target_i", C.c_int * 9),
-                ("target_j", C.c_int * 9), ("target_v", C.c_double * 9)]
+                ("target_j", C.c_int * 9), ("target_v", C.c_double * 9), ("catalog_type", C.c_int),
+                ("barrier_per_voxel", C.c_int)]
+
+
+CATALOG_TYPES = {"random": 0, "even": 1, "fibonacci": 2}
 
 
 def params_from_config(cfg) -> KmcParams:
@@ -91,6 +95,8 @@ def params_from_config(cfg) -> KmcParams:
     p.redraw_barriers, p.use_3d_barriers = int(cfg.redraw_barriers), int(cfg.use_3d_barriers)
     p.step_size, p.mixed_tol, p.max_kmc_steps_pct = cfg.step_size, cfg.mixed_tol_pa, cfg.max_kmc_steps_pct
     p.comp_i, p.comp_j = cfg.driving
+    p.catalog_type = CATALOG_TYPES[cfg.catalog_type]
+    p.barrier_per_voxel = int(cfg.barrier_per_voxel)
     tg = sorted(cfg.targets.items())
     p.n_targets = len(tg)
     for k, ((i, j), v) in enumerate(tg):
@@ -135,6 +141,8 @@ class OracleKmc:
         E = np.ascontiguousarray(cfg.E, dtype=np.float64)
         nu = np.ascontiguousarray(cfg.nu, dtype=np.float64)
         self.h = lib().oracle_kmc_create(C.byref(self.p), _dp(E), _dp(nu))
+        if not self.h:
+            raise ValueError("the oracle refused the configuration (fibonacci catalogs need 3D)")
 
     def __del__(self):
         if getattr(self, "h", None):
