@@ -14,8 +14,9 @@ modulus field, CoV 0.10, correlation 4 voxels, M = 18 modes per voxel).
 
 * ``value`` -- the chosen form: the four replicas advanced together by the
   batched, device-resident kernel (mgk_batch_run), K thermal events each;
-  CUDA-event time of the launch.  ``e2e``: the same through the public call
-  with its host<->device copies, wall clock.
+  CUDA-event time of the launch.  ``e2e``: the same call (the same events)
+  timed by the wall clock through the public API, its host<->device copies
+  and the replicas' macroscopic results read back included.
 * ``plain`` -- the drop-in form (mgk_kmc_run, one replica at a time, host RNG
   replay), K events of seed 0, CUDA-event time of the run; its ``e2e``
   through the public API with every step's copies.
@@ -145,12 +146,34 @@ def batch_traffic_from_profiles(workload: str, events: float):
     return float(m.group(1)) * events if m else None
 
 
+def host_cpu():
+    """CPU model and whether it runs the AVX2/FMA build of the reference."""
+    model, flags = "unknown", set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and model == "unknown":
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags") and not flags:
+                    flags = set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return model, {"avx2", "fma", "bmi2"} <= flags
+
+
 def run_reference(cfg_paths, n_events: int, timeout: float = 900.0):
-    """Time the reference's own CPU path (oracle/_ref/ref_driver kmc_trace):
-    the first n_events thermal events of every workload in cfg_paths, one
-    process each, all at once; setup excluded.  Returns the aggregate rate
-    (events of all processes / the slowest process's loop time)."""
-    drv = os.path.join(HERE, "oracle", "_ref", "ref_driver")
+    """Time the reference's own CPU path (the unmodified reference headers
+    driven by oracle/_ref/ref_driver kmc_trace; its -O3 AVX2 build
+    ref_driver_o3 where the host runs it): the first n_events thermal events of
+    every workload in cfg_paths, one process each, all at once; setup
+    excluded.  Returns the aggregate rate (events of all processes / the
+    slowest process's loop time)."""
+    model, v3 = host_cpu()
+    drv = os.path.join(HERE, "oracle", "_ref", "ref_driver_o3")
+    build = "-O3 -march=x86-64-v3"
+    if not (v3 and os.path.exists(drv)):
+        drv = os.path.join(HERE, "oracle", "_ref", "ref_driver")
+        build = "-O2 -ffp-contract=off"
     if not os.path.exists(drv):
         return None, "oracle/_ref/ref_driver not built"
     dirs = [tempfile.mkdtemp(prefix="mgk_ref_") for _ in cfg_paths]
@@ -175,7 +198,8 @@ def run_reference(cfg_paths, n_events: int, timeout: float = 900.0):
         vals = open(os.path.join(d, "timing.txt")).read().split()
         nev += int(float(vals[1]))
         secs = max(secs, float(vals[2]))
-    return {"events": nev, "seconds": secs, "value": nev / secs if secs > 0 else 0.0, "processes": len(cfg_paths)}, None
+    return {"events": nev, "seconds": secs, "value": nev / secs if secs > 0 else 0.0, "processes": len(cfg_paths),
+            "cpu": model, "binary": os.path.basename(drv), "build": build}, None
 
 
 def reduce_over_ranks(dist, seconds: float, events: float, device=None):
@@ -235,10 +259,12 @@ def ensemble_block(G, workloads, workdir, seconds, plain_events):
     vox_iters = sum(x["ls_iters"] * c.n_voxels for x, c in zip(st, cfgs))
     lat = np.concatenate([x["event_us"] for x in st if len(x["event_us"])]) if events else np.zeros(0)
     classes = {}
+    rep_rate = []
     for name, x in zip(ENSEMBLE, st):
         k = classes.setdefault(name, {"replicas": 0, "events": 0, "ctas": int(x["ctas"])})
         k["replicas"] += 1
         k["events"] += int(x["events"])
+        rep_rate.append((name, x["events"] / (ms / 1e3) if ms > 0 else 0.0))
     b.close()
     # plain form, replica by replica: per-class rate on the class's first replica
     kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
@@ -260,13 +286,27 @@ def ensemble_block(G, workloads, workdir, seconds, plain_events):
         del sim
     chosen = events / (ms / 1e3) if ms > 0 else 0.0
     plain = events / plain_time if plain_time > 0 else None
+    # per class: the class's events per second in the batch against the plain
+    # form's per-replica rate (what running the class's replicas one after
+    # another would give); makespan: the time for every replica to advance
+    # 20 events, in the batch (its slowest replica) and replica by replica
+    for k in classes.values():
+        k["batch_steps_per_s"] = k["events"] / (ms / 1e3) if ms > 0 else 0.0
+        p = k.get("plain_steps_per_s") or 0.0
+        k["speedup_vs_plain"] = k["batch_steps_per_s"] / p if p > 0 else None
+    K = 20
+    mk_batch = max((K / r for _, r in rep_rate if r > 0), default=None)
+    mk_plain = sum(K / classes[n]["plain_steps_per_s"] for n, _ in rep_rate
+                   if classes[n].get("plain_steps_per_s"))
+    makespan = {"events_per_replica": K, "batch_s": mk_batch, "plain_replica_by_replica_s": mk_plain,
+                "speedup": (mk_plain / mk_batch) if mk_batch else None}
     return {"replicas": len(cfgs), "composition": "16x2D 64^2, 16x2D 128^2, 16x2D 512^2, 5x3D 32^3, 5x3D 48^3, "
                                                 "6x3D 96^3 (M 18 in 2D, 100 in 3D)",
             "device_seconds": ms / 1e3, "events": int(events), "value": chosen, "unit": UNIT,
             "ls_voxel_iterations_per_s": vox_iters / (ms / 1e3) if ms > 0 else None,
             "plain_replica_by_replica": plain, "speedup_vs_plain": (chosen / plain) if plain else None,
             "latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},
-            "per_class": classes, "setup_seconds": t_setup}
+            "per_class": classes, "makespan": makespan, "setup_seconds": t_setup}
 
 
 # algorithmic bytes of one LS iteration per voxel with an FP32 spectrum: the
@@ -408,7 +448,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded lognormal modulus fields)", "config": base_cfg,
                 "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": len(cfg_paths), "kind": "reference",
-                                 "sample": sample},
+                                 "sample": sample, "cpu": res["cpu"], "binary": res["binary"], "build": res["build"]},
                 "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -440,13 +480,21 @@ def main():
     # chosen form: all replicas in one device-resident launch
     progress("chosen form: %d replicas" % len(cfgs))
     batch = G.KmcBatch(cfgs)
-    batch.run(args.warmup)
+    # clocks sampled from the warm-up to the end of the plain form's timed run
     clocks = ClockSampler(local_rank)
     clocks.start()
+    batch.run(args.warmup)
     barrier()
+    # one public call: its launch is timed on the device (value) and the
+    # whole call -- control blocks and generator states to the device, the
+    # launch, counters, states, selections and event times back -- plus every
+    # replica's macroscopic result read back, by the wall clock (e2e): the
+    # same events for both
+    t0 = time.perf_counter()
     ms = batch.run(args.steps)
+    macros = [batch.macro(r) for r in range(len(cfgs))]
     barrier()
-    clk = clocks.stop()
+    t_e2e = time.perf_counter() - t0
     st = [batch.stats(r) for r in range(len(cfgs))]
     ev = sum(x["events"] for x in st)
     t_chosen, ev_all = reduce_over_ranks(dist, ms / 1e3, ev, dev)
@@ -454,20 +502,10 @@ def main():
     lat = np.concatenate([x["event_us"] for x in st])
     iters = sum(x["ls_iters"] for x in st)
     sweeps = sum(x["sweeps"] for x in st)
-    # e2e of the chosen form: the public call (its control blocks and
-    # generator states to the device, counters, generator states, selections
-    # and event times back) plus every replica's macroscopic result read back
-    barrier()
-    t0 = time.perf_counter()
-    batch.run(args.steps)
-    macros = [batch.macro(r) for r in range(len(cfgs))]
-    barrier()
-    t_e2e = time.perf_counter() - t0
-    st2 = [batch.stats(r) for r in range(len(cfgs))]
-    ev2 = sum(x["events"] for x in st2)
-    h2d = sum(x["h2d_bytes"] for x in st2)
-    d2h = sum(x["d2h_bytes"] for x in st2) + sum(m.nbytes for m in macros)
-    t_e2e, ev2_all = reduce_over_ranks(dist, t_e2e, ev2, dev)
+    h2d = sum(x["h2d_bytes"] for x in st)
+    d2h = sum(x["d2h_bytes"] for x in st) + sum(m.nbytes for m in macros)
+    t_e2e, ev2_all = reduce_over_ranks(dist, t_e2e, ev, dev)
+    ev2 = ev
     e2e_value = ev2_all / t_e2e if t_e2e > 0 else 0.0
     batch.close()
 
@@ -483,22 +521,28 @@ def main():
     sim.set_profiling(True)
     p0 = sim.stats
     barrier()
-    segment(args.steps)
-    barrier()
-    prof = sim.profile()
-    p1 = sim.stats
-    pev = p1["thermal_events"] - p0["thermal_events"]
-    t_plain, pev_all = reduce_over_ranks(dist, prof["run_ms"] / 1e3, pev, dev)
-    plain_value = pev_all / t_plain if t_plain > 0 else 0.0
-    sim.set_profiling(False)
-    barrier()
+    # the same segment timed on the device (its launches' CUDA events) and by
+    # the wall clock through the public API (host RNG draws and every step's
+    # copies included)
     t0 = time.perf_counter()
     segment(args.steps)
     barrier()
     tp_e2e = time.perf_counter() - t0
-    p2 = sim.stats
-    tp_e2e, pev2 = reduce_over_ranks(dist, tp_e2e, p2["thermal_events"] - p1["thermal_events"], dev)
+    prof = sim.profile()
+    p1 = sim.stats
+    clk = clocks.stop()
+    pev = p1["thermal_events"] - p0["thermal_events"]
+    t_plain, pev_all = reduce_over_ranks(dist, prof["run_ms"] / 1e3, pev, dev)
+    plain_value = pev_all / t_plain if t_plain > 0 else 0.0
+    tp_e2e, pev2 = reduce_over_ranks(dist, tp_e2e, pev, dev)
     plain_e2e = pev2 / tp_e2e if tp_e2e > 0 else 0.0
+    sim.set_profiling(False)
+    # the pass plan the LS autotuner picks for this grid (standalone solver)
+    try:
+        grid = (cfg.nx, cfg.ny) if cfg.dim == 2 else (cfg.nx, cfg.ny, cfg.nz)
+        ls_plan = G.LsSolver(grid, cfg.E, cfg.nu).plan()
+    except Exception as e:  # reported, not fatal
+        ls_plan = {"error": str(e)[-200:]}
     del sim
 
     ens = None
@@ -541,6 +585,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": 1e3 * t_chosen / max(ev, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lognormal modulus fields)",
             "config": dict(base_cfg, ls_iterations_per_step=iters / max(ev, 1), sweeps_per_step=sweeps / max(ev, 1),
+                           ls_plan=ls_plan,
                            ctas_per_replica=[int(x["ctas"]) for x in st],
                            phase_ms={k[3:]: round(sum(x[k] for x in st) / len(st), 3) for k in st[0] if k.startswith("ms_")}),
             "latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99),
@@ -578,6 +623,7 @@ def main():
         res, err = run_reference(cfg_paths, args.cpu_events)
         if res is not None:
             line["cpu_baseline"] = {"value": res["value"], "unit": UNIT, "cores": len(cfg_paths), "kind": "reference",
+                                    "cpu": res["cpu"], "binary": res["binary"], "build": res["build"],
                                     "sample": "first %d thermal events of each replica of the same workload, one "
                                               "reference process (oracle/_ref/ref_driver) per replica run "
                                               "concurrently, setup excluded" % args.cpu_events}

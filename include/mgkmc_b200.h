@@ -156,6 +156,12 @@ typedef struct {
      * as one value after a flip). */
     int catalog_type;
     int barrier_per_voxel;
+    /* No counterpart in the reference: arithmetic of the LS re-solves
+     * (elastic_run), 0 FP64 (the reference's), 1 FP32-refined (FP32 spectrum,
+     * FFTs and Green operator to a relative change of max(ls_tol, 1e-6), then
+     * FP64 iterations from that field to ls_tol), in both the plain and the
+     * batched form. */
+    int ls_precision;
 } mgk_kmc_params;
 
 /* run_simulation arguments (kmc_solver.hpp:721-729) plus a thermal-event cap. */

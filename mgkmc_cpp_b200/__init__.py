@@ -158,7 +158,8 @@ class _KmcBase:
     def _create(self, nx, ny, nz, M, gamma0, E_field, nu_field, pixel, barrier_gen, softening_scheme, softening_cap, jp,
                 jt, neighbor_softening_fraction, q_act_temp, output_dir, temperature, strain_rate, stability_threshold,
                 nu0, plane_mode, fast_patching_enabled, patch_radius, sync_interval, instability_mode, cascade_timing,
-                scale_rate_by_volume, redraw_directions, redraw_barriers, use_3d_barriers, seed, ls_tol, ls_max_iter):
+                scale_rate_by_volume, redraw_directions, redraw_barriers, use_3d_barriers, seed, ls_tol, ls_max_iter,
+                catalog_type="random", barrier_per_voxel=False, ls_precision="fp64"):
         L = _lib.lib()
         _lib.require_device()
         self.nx, self.ny, self.nz, self.M = nx, ny, nz, M
@@ -184,6 +185,11 @@ class _KmcBase:
         p.use_3d_barriers = int(bool(use_3d_barriers))
         p.fast_patching, p.patch_radius, p.sync_interval = int(bool(fast_patching_enabled)), patch_radius, sync_interval
         p.ls_tol, p.ls_max_iter = float(ls_tol), int(ls_max_iter)
+        if catalog_type not in ("random", "even", "fibonacci") or ls_precision not in ("fp64", "fp32_refined"):
+            raise ValueError("catalog_type: random | even | fibonacci; ls_precision: fp64 | fp32_refined")
+        p.catalog_type = {"random": 0, "even": 1, "fibonacci": 2}[catalog_type]
+        p.barrier_per_voxel = int(bool(barrier_per_voxel))
+        p.ls_precision = 1 if ls_precision == "fp32_refined" else 0
         self._params = p
         E = np.ascontiguousarray(E_field, dtype=np.float64).reshape(-1)
         nu = np.ascontiguousarray(nu_field, dtype=np.float64).reshape(-1)
@@ -307,12 +313,15 @@ class KmcSimulation2D(_KmcBase):
                  output_dir="output", temperature=0.0, strain_rate=1.0, stability_threshold=0.0, nu0=1e13,
                  plane_mode="plane_strain", fast_patching_enabled=False, patch_radius=5, sync_interval=100,
                  instability_mode="cascade", cascade_timing="none", scale_rate_by_volume=True, redraw_directions=True,
-                 redraw_barriers=True, seed=42, ls_tol=1e-6, ls_max_iter=200):
+                 redraw_barriers=True, seed=42, ls_tol=1e-6, ls_max_iter=200, **ext):
+        """The reference constructor's arguments; ``ext`` takes the extensions
+        with no counterpart in the reference: catalog_type ("random" |
+        "even"), barrier_per_voxel, ls_precision ("fp64" | "fp32_refined")."""
         self._create(nx, ny, 1, M, gamma0, E_field, nu_field, pixel, barrier_gen, softening_scheme, softening_cap, jp, jt,
                      neighbor_softening_fraction, q_act_temp, output_dir, temperature, strain_rate, stability_threshold,
                      nu0, plane_mode, fast_patching_enabled, patch_radius, sync_interval, instability_mode,
                      cascade_timing, scale_rate_by_volume, redraw_directions, redraw_barriers, False, seed, ls_tol,
-                     ls_max_iter)
+                     ls_max_iter, **ext)
 
 
 class KmcSimulation3D(_KmcBase):
@@ -324,12 +333,16 @@ class KmcSimulation3D(_KmcBase):
                  q_act_temp=0.37, output_dir="output", temperature=0.0, strain_rate=1.0, stability_threshold=0.0,
                  nu0=1e13, fast_patching_enabled=False, patch_radius=5, sync_interval=100, instability_mode="cascade",
                  cascade_timing="none", scale_rate_by_volume=True, redraw_directions=True, redraw_barriers=True,
-                 use_3d_barriers=False, seed=42, ls_tol=1e-6, ls_max_iter=200):
+                 use_3d_barriers=False, seed=42, ls_tol=1e-6, ls_max_iter=200, **ext):
+        """The reference constructor's arguments; ``ext`` takes the extensions
+        with no counterpart in the reference: catalog_type ("random" | "even"
+        | "fibonacci"), barrier_per_voxel, ls_precision ("fp64" |
+        "fp32_refined")."""
         self._create(nx, ny, nz, M, gamma0, E_field, nu_field, pixel, barrier_gen, softening_scheme, softening_cap, jp,
                      jt, neighbor_softening_fraction, q_act_temp, output_dir, temperature, strain_rate,
                      stability_threshold, nu0, "plane_strain", fast_patching_enabled, patch_radius, sync_interval,
                      instability_mode, cascade_timing, scale_rate_by_volume, redraw_directions, redraw_barriers,
-                     use_3d_barriers, seed, ls_tol, ls_max_iter)
+                     use_3d_barriers, seed, ls_tol, ls_max_iter, **ext)
 
 
 def from_config(cfg, output_dir: Optional[str] = None):
@@ -344,7 +357,8 @@ def from_config(cfg, output_dir: Optional[str] = None):
               sync_interval=cfg.sync_interval, instability_mode=cfg.instability_mode,
               cascade_timing=cfg.cascade_timing, scale_rate_by_volume=cfg.scale_rate_by_volume,
               redraw_directions=cfg.redraw_directions, redraw_barriers=cfg.redraw_barriers, seed=cfg.seed,
-              ls_tol=cfg.ls_tol, ls_max_iter=cfg.ls_max_iter)
+              ls_tol=cfg.ls_tol, ls_max_iter=cfg.ls_max_iter, catalog_type=cfg.catalog_type,
+              barrier_per_voxel=cfg.barrier_per_voxel, ls_precision=cfg.ls_precision)
     if cfg.dim == 3:
         sim = KmcSimulation3D(cfg.nx, cfg.ny, cfg.nz, cfg.M, cfg.gamma0, cfg.E, cfg.nu,
                               use_3d_barriers=cfg.use_3d_barriers, **kw)
@@ -581,6 +595,7 @@ def kmc_params_from_config(cfg) -> "_lib.KmcParamsC":
     p.ls_tol, p.ls_max_iter = float(cfg.ls_tol), int(cfg.ls_max_iter)
     p.catalog_type = {"random": 0, "even": 1, "fibonacci": 2}[cfg.catalog_type]
     p.barrier_per_voxel = int(cfg.barrier_per_voxel)
+    p.ls_precision = 1 if cfg.ls_precision == "fp32_refined" else 0
     return p
 
 

@@ -42,7 +42,8 @@ class KmcParamsC(C.Structure):
                 ("instability_kmc", C.c_int), ("scale_rate_by_volume", C.c_int), ("redraw_directions", C.c_int),
                 ("redraw_barriers", C.c_int), ("use_3d_barriers", C.c_int), ("fast_patching", C.c_int),
                 ("patch_radius", C.c_int), ("sync_interval", C.c_int), ("ls_tol", C.c_double),
-                ("ls_max_iter", C.c_int), ("catalog_type", C.c_int), ("barrier_per_voxel", C.c_int)]
+                ("ls_max_iter", C.c_int), ("catalog_type", C.c_int), ("barrier_per_voxel", C.c_int),
+                ("ls_precision", C.c_int)]
 
 
 class LeParamsC(C.Structure):

@@ -7,8 +7,8 @@ by indentation, leaves are stripped of one pair of quotes, there are no lists.
 including the GPa -> Pa auto-conversion (main.cpp:61-64, 96-99, 349-351) and the
 driving-component / mixed-target parsing (main.cpp:319-375).  Keys the reference
 never reads are ignored, as there.  New keys of this build live under new names
-(``ls.tol``, ``ls.max_iter``, ``run.max_flips``) and default to the reference's
-hard-coded values.  Two keys select extensions with no counterpart in the
+(``ls.tol``, ``ls.max_iter``, ``ls.precision``, ``run.max_flips``) and default
+to the reference's hard-coded values.  Two keys select extensions with no counterpart in the
 reference (defaults: the reference's behaviour):
 
 * ``catalog.type``: ``random`` (the reference's modes, kmc_solver.hpp:231-238,
@@ -219,6 +219,7 @@ class SimConfig:
     max_flips: int = -1
     catalog_type: str = "random"
     barrier_per_voxel: bool = False
+    ls_precision: str = "fp64"
     output_directory: str = "simulation_results"
     summary_filename: str = "summary_log.txt"
     enable_console: bool = True
@@ -313,6 +314,9 @@ class SimConfig:
         if s.catalog_type == "fibonacci" and s.dim != 3:
             raise ValueError("catalog.type fibonacci needs a 3D system")
         s.barrier_per_voxel = c.get_bool("barriers.per_voxel", False)
+        s.ls_precision = c.get_string("ls.precision", "fp64").lower()
+        if s.ls_precision not in ("fp64", "fp32_refined"):
+            raise ValueError("ls.precision must be fp64 or fp32_refined")
         return s
 
 

@@ -65,6 +65,7 @@ struct BatchRep {
     double gamma0;
     int redraw_dir, redraw_bar, C, pad0;
     int ext, rd_dir, rd_bar, pad1;  // catalog / per-voxel barrier extensions and their RD_* redraw modes
+    int ls_prec, pad2;              // LS re-solves: 0 FP64, 1 FP32-refined
     int ncta;
     unsigned* bar;  // {arrivals, generation, error, spare}
     dd* chunk_sum;
@@ -128,11 +129,32 @@ MGK_DEV bool group_solve(BatchRep& R, int rank, const GridBar& gb, unsigned char
             for (int k = 0; k < 3; ++k) c->w[k] = wbar[k];
     }
     __syncthreads();
+    int it32 = 0;
+    if (R.ls_prec == 1 && c->ls_max_iter > 1) {
+        // FP32 phase (FP32 spectrum, FFTs and Green operator; real-space
+        // fields, norms and sums in FP64) to a relative change of
+        // max(tol, kFp32Tol), then the FP64 phase below from that field: a
+        // warm start whose mean is already eps_bar (LsSolver::solve's scheme)
+        __shared__ LsArgs s32;
+        if (threadIdx.x == 0) {
+            s32 = *sls;
+            s32.tol = fmax(sls->tol, kFp32Tol);
+            s32.max_iter = sls->max_iter - 1;
+        }
+        __syncthreads();
+        if (!lsdev::ls_solve_group<D, float>(s32, rank, R.ncta, gb, smem)) return false;
+        if (threadIdx.x == 0) {
+            it32 = s32.result->iters;
+            sls->norm_extra_first = sls->norm_extra;
+            sls->diff_extra_first = 0.0;
+        }
+        __syncthreads();
+    }
     if (!lsdev::ls_solve_group<D, double>(*sls, rank, R.ncta, gb, smem)) return false;
     if (rank == 0 && threadIdx.x == 0) {
         macro_from_result<D>(sls->result, c, c->w, R.s.N);
         c->ls_solves++;
-        c->ls_iters += sls->result->iters;
+        c->ls_iters += sls->result->iters + it32;
     }
     return true;
 }
@@ -1104,6 +1126,7 @@ void BatchEngine::init() {
         R.redraw_dir = e.p_.redraw_directions;
         R.redraw_bar = e.p_.redraw_barriers;
         R.ext = e.p_.catalog_type != 0 || e.p_.barrier_per_voxel;
+        R.ls_prec = e.p_.ls_precision;
         R.rd_dir = e.rd_dir_;
         R.rd_bar = e.rd_bar_;
         R.C = e.C_;

@@ -101,6 +101,8 @@ KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu)
     CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     int dims[3] = {p.nx, p.ny, D_ == 3 ? p.nz : 1};
     ls_.reset(new LsSolver(D_, dims, p.plane_stress != 0, p.pixel, E, nu, st_));
+    if (p.ls_precision < 0 || p.ls_precision > 1) throw std::invalid_argument("ls_precision must be 0 or 1");
+    ls_->set_precision(p.ls_precision);
     bar_.type = p.barrier_type;
     bar_.mean = p.bar_mean;
     bar_.std_val = p.bar_std;

@@ -323,70 +323,28 @@ MGK_DEV void publish_partials(const LsArgs& a, int cta, double* part, double* re
         for (int k = 0; k < NP; ++k) a.partials[cta * kMaxPartials + k] = part[k];
 }
 
-// Group barrier that also sums the CTAs' partials (publish_partials): the last
-// CTA to arrive adds them in a fixed order -- thread t sums value (t & 15)
-// over CTAs (t >> 4), (t >> 4) + 16, ..., then the 16 group sums are added
-// in group order, the same bits whichever CTA arrives last -- writes the sums
-// to a.red and releases the others, which read them there.  `out` (shared,
-// NP values) gets the sums in every CTA.  256 threads per CTA.  Bounded like
-// grid_sync; returns false when a wait gave up.
+// Every CTA reduces all partials in the same fixed order -> identical values:
+// thread t sums value (t & 15) over CTAs (t >> 4), (t >> 4) + 16, ..., then
+// the 16 group sums are added in group order.  256 threads per CTA.  (Reducing
+// once, in the last CTA to reach the barrier, and reading the sums back was
+// measured slower: one more L2 round trip on the critical path.)
 template <int NP>
-MGK_DEV bool grid_sync_reduce(const LsArgs& a, const GridBar& g, int ncta, double* out) {
+MGK_DEV void gather_partials(const LsArgs& a, int ncta, double* out /* shared, NP */) {
     __shared__ double grp[256];
-    __shared__ int s_last, s_ok;
-    __shared__ unsigned s_gen;
+    const int k = threadIdx.x & 15, g = threadIdx.x >> 4;
+    double s = 0.0;
+    if (k < NP) {
+#pragma unroll 4
+        for (int b = g; b < ncta; b += 16) s += __ldcg(&a.partials[b * kMaxPartials + k]);
+    }
+    grp[threadIdx.x] = s;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* gen = g.bar + 1;
-        s_gen = *gen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(g.bar, 1u);
-        s_last = arrived == g.nblocks - 1;
-        s_ok = 1;
+    if (threadIdx.x < NP) {
+        double t = 0.0;
+        for (int gg = 0; gg < 16; ++gg) t += grp[gg * 16 + threadIdx.x];
+        out[threadIdx.x] = t;
     }
     __syncthreads();
-    if (s_last) {
-        const int k = threadIdx.x & 15, gg = threadIdx.x >> 4;
-        double sum = 0.0;
-        if (k < NP)
-            for (int b = gg; b < ncta; b += 16) sum += __ldcg(&a.partials[b * kMaxPartials + k]);
-        grp[threadIdx.x] = sum;
-        __syncthreads();
-        if (threadIdx.x < NP) {
-            double t = 0.0;
-            for (int q = 0; q < 16; ++q) t += grp[q * 16 + threadIdx.x];
-            __stcg(&a.red[threadIdx.x], t);
-            out[threadIdx.x] = t;
-            __threadfence();
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            atomicExch(g.bar, 0u);
-            __threadfence();
-            atomicAdd(g.bar + 1, 1u);
-        }
-    } else {
-        if (threadIdx.x == 0) {
-            volatile unsigned* gen = g.bar + 1;
-            const unsigned long long t0 = global_ns();
-            unsigned polls = 0;
-            while (*gen == s_gen) {
-                __nanosleep(32);
-                if ((*(volatile unsigned*)g.err & MGK_DERR_BARRIER_TIMEOUT) ||
-                    ((++polls & 255u) == 0 && global_ns() - t0 > g.limit_ns)) {
-                    atomicOr(g.err, MGK_DERR_BARRIER_TIMEOUT);
-                    s_ok = 0;
-                    break;
-                }
-            }
-            __threadfence();
-        }
-        __syncthreads();
-        if (s_ok && threadIdx.x < NP) out[threadIdx.x] = __ldcg(&a.red[threadIdx.x]);
-    }
-    if (threadIdx.x == 0 && (*(volatile unsigned*)g.err & MGK_DERR_BARRIER_TIMEOUT)) s_ok = 0;
-    __syncthreads();
-    return s_ok != 0;
 }
 
 // One LS solve by a group of ncta co-resident CTAs (rank cta), synchronised by
@@ -394,7 +352,7 @@ MGK_DEV bool grid_sync_reduce(const LsArgs& a, const GridBar& g, int ncta, doubl
 // pass layout of pass_smem).  The result goes to a.result.  Returns false
 // when a barrier wait gave up (the error word is set).
 template <int D, typename T>
-MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& gb, unsigned char* smem_raw) {
+__device__ __noinline__ bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& gb, unsigned char* smem_raw) {
     constexpr int S = D == 2 ? 3 : 6;
     constexpr int NP = 2 + 2 * S;
     __shared__ double red[14 * 32];
@@ -417,18 +375,22 @@ MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& g
                 for (int c = 0; c < S; ++c) acc[c] += a.eps_s[(long)c * a.N + v];
         }
         publish_partials<NP>(a, cta, acc, red);
-        if (!grid_sync_reduce<NP>(a, gb, ncta, vals)) return false;
+        if (!grid_sync(gb)) return false;
+        gather_partials<NP>(a, ncta, vals);
         if (threadIdx.x < S) s_shift[threadIdx.x] = a.ebar_s[threadIdx.x] - vals[threadIdx.x] * a.inv_n;
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < S; ++c) shift[c] = s_shift[c];
+        // the row pass below publishes new partials: every CTA must have read these first
+        if (!grid_sync(gb)) return false;
     }
     double part[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) part[k] = 0.0;
     row_pass<D, T, 0>(a, cta, ncta, smem_raw, part, shift);
     publish_partials<NP>(a, cta, part, red);
-    if (!grid_sync_reduce<NP>(a, gb, ncta, vals)) return false;
+    if (!grid_sync(gb)) return false;
+        gather_partials<NP>(a, ncta, vals);
     int it = 0;
     double diff = 0.0;
     while (it < a.max_iter) {
@@ -446,7 +408,8 @@ MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& g
         for (int k = 0; k < NP; ++k) part[k] = 0.0;
         row_pass<D, T, 1>(a, cta, ncta, smem_raw, part, shift);
         publish_partials<NP>(a, cta, part, red);
-        if (!grid_sync_reduce<NP>(a, gb, ncta, vals)) return false;
+        if (!grid_sync(gb)) return false;
+        gather_partials<NP>(a, ncta, vals);
         const double dx = it == 0 ? a.diff_extra_first : 0.0;
         const double nx = it == 0 ? a.norm_extra_first : a.norm_extra;
         ++it;

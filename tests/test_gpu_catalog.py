@@ -77,7 +77,8 @@ CASES = {
     "even2d_noredraw": dict(rdir="false", rbar="false", seed=7, soft="true", scheme="directional"),
     "random2d_voxel": dict(cat="random", M=4, nx=10, ny=10, seed=9),
     "random2d_voxel_dironly": dict(cat="random", M=4, nx=10, ny=10, rbar="false", seed=11),
-    "even3d_mode": dict(dim="3d", nx=6, ny=6, nz=4, M=4, pv="false", drive="zz", targets=_T3, seed=13),
+    "even3d_mode": dict(dim="3d", nx=6, ny=6, nz=4, M=4, pv="false", drive="xx", targets="    yy: 0.0\n    zz: 0.0",
+                        seed=13),
     "fib3d_voxel": dict(dim="3d", nx=8, ny=8, nz=8, M=10, cat="fibonacci", drive="zz", targets=_T3, seed=15,
                         soft="true", scheme="directional"),
     "fib3d_mode": dict(dim="3d", nx=6, ny=8, nz=5, M=7, cat="fibonacci", pv="false", drive="zz", targets=_T3,
