@@ -354,7 +354,7 @@ def precision_block(G, cases=(((512, 512), 11), ((64, 64, 64), 12)), solves=3):
     return out
 
 
-def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05):
+def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05, plain_events=20):
     """The serving loop on a Poisson request stream (20 jobs/s, seed 7): jobs
     are admitted as they arrive (wall clock) and as memory allows, every
     active job advances in shared batched launches of slice_seconds of device
@@ -378,13 +378,40 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05)
     wall = time.perf_counter() - t0
     done = list(srv.done.values())
     events = sum(j["events"] for j in done)
-    stalled = sum(1 for j in done if j["stalled"])
+    stalled = [j for j in done if j["stalled"]]
+    terminated = [j for j in done if not j["stalled"] and j["events"] < j["target"]]
     comp = [j["finished"] - j["arrival"] for j in done]
     lat = np.array(srv.step_latency_us)
+    # the plain form on the same job stream: each size class's rate on its
+    # first job (plain_events events after 3 of warm-up), every job's events
+    # at its class's rate, one job after another
+    kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
+    rates = {}
+    for _, cfg, _ in jobs:
+        key = (cfg.dim, cfg.nx)
+        if key in rates:
+            continue
+        sim = G.from_config(cfg, output_dir=None)
+        sim.run_simulation(10 ** 6, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50, max_events=3, **kw)
+        sim.set_profiling(True)
+        e0 = sim.stats["thermal_events"]
+        sim.run_simulation(10 ** 6, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50,
+                           max_events=plain_events, **kw)
+        ev = sim.stats["thermal_events"] - e0
+        rates[key] = ev / (sim.profile()["run_ms"] / 1e3) if ev else 0.0
+        del sim
+    plain_s = sum(j["events"] / rates[(j["cfg"].dim, j["cfg"].nx)] for j in done
+                  if rates.get((j["cfg"].dim, j["cfg"].nx)))
     return {"jobs": len(done), "arrivals": "Poisson 20 jobs/s, seed 7", "flips_per_job": list(flips),
             "sizes": ["%s %d" % x for x in sizes], "slice_seconds": slice_seconds, "events": int(events),
-            "wall_seconds": wall, "device_seconds": dev_ms / 1e3, "launches": srv.launches, "stalled_jobs": stalled,
+            "wall_seconds": wall, "device_seconds": dev_ms / 1e3, "launches": srv.launches,
+            "stalled_jobs": len(stalled), "stalled_why": "no thermal event for %.0f s of device time (an avalanche "
+                                                        "whose cascade batches never settle)" % srv.stall_seconds,
+            "terminated_jobs": len(terminated),
             "value": events / wall if wall > 0 else None, "unit": UNIT,
+            "plain_job_by_job_seconds": plain_s, "plain_steps_per_s": events / plain_s if plain_s > 0 else None,
+            "speedup_vs_plain": (events / wall) / (events / plain_s) if plain_s > 0 and wall > 0 else None,
+            "plain_rates_by_class": {"%dD %d" % k: v for k, v in rates.items()},
             "step_latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},
             "job_completion_s": {"p50": percentile(comp, 50), "p99": percentile(comp, 99)}}
 
@@ -404,6 +431,8 @@ def main():
     ap.add_argument("--only-precision", action="store_true",
                     help="run only the FP64 / FP32-refined LS block and print its JSON (profiling the LS kernels)")
     ap.add_argument("--ensemble-seconds", type=float, default=40.0)
+    ap.add_argument("--ensemble-plan", default="throughput", choices=["throughput", "balanced"],
+                    help="how the ensemble's batch spreads CTAs over the replicas (mgk_set_batch_plan)")
     ap.add_argument("--serve-jobs", type=int, default=40, help="jobs of the serving block (0: skip)")
     ap.add_argument("--serve-flips", type=int, nargs=2, default=[50, 500])
     ap.add_argument("--serve-full-sizes", action="store_true",
@@ -549,7 +578,10 @@ def main():
     progress("ensemble")
     if not args.no_ensemble and rank == 0:
         try:
+            G.set_batch_plan(args.ensemble_plan)
             ens = ensemble_block(G, workloads, workdir, args.ensemble_seconds, 20)
+            ens["plan"] = args.ensemble_plan
+            G.set_batch_plan("throughput")
         except Exception as e:  # reported, never silently dropped
             ens = {"error": str(e)[-300:]}
     prec = None

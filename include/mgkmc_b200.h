@@ -292,6 +292,13 @@ MGK_API mgk_status mgk_batch_get_macro(mgk_batch* h, int replica, double* out, i
  * into us; *len gets the count.  No counterpart in the reference. */
 MGK_API mgk_status mgk_batch_event_times(mgk_batch* h, int replica, double* us, long long cap, long long* len);
 MGK_API mgk_status mgk_batch_set_time_limit(mgk_batch* h, double seconds);
+/* No counterpart in the reference.  How batches created from now on spread
+ * their CTAs over the replicas: 0 (default) throughput -- each CTA goes to the
+ * replica whose modelled event rate it raises most, so small latency-bound
+ * grids get most; 1 balanced -- each CTA goes to the replica furthest below
+ * the rate it would have on the whole GPU, so that mixed sizes advance at
+ * similar fractions of their single-replica speed (shorter makespan). */
+MGK_API mgk_status mgk_set_batch_plan(int objective);
 MGK_API void mgk_batch_destroy(mgk_batch* h);
 
 /* Measurement hooks (no counterpart in the reference, which only logs wall

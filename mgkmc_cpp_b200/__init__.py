@@ -618,6 +618,12 @@ def run_params_from_config(cfg, n_global_steps=None, max_cascade_batches=0) -> "
     return rp
 
 
+def set_batch_plan(objective: str):
+    """How batches built from now on spread their CTAs: "throughput" (default)
+    or "balanced" (see mgk_set_batch_plan)."""
+    _lib.check(_lib.lib().mgk_set_batch_plan({"throughput": 0, "balanced": 1}[objective]))
+
+
 class KmcBatch:
     """Replicas advanced together by one device-resident kernel (mgk_batch_*):
     no host round trip per event; the reference's random stream continued on

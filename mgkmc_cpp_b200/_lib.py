@@ -20,7 +20,7 @@ EXPORTS = ["mgk_last_error", "mgk_version", "mgk_device_count", "mgk_ls_create",
            "mgk_kmc_destroy", "mgk_kmc_set_profiling", "mgk_kmc_get_profile", "mgk_batch_create", "mgk_batch_run",
            "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro", "mgk_batch_set_time_limit", "mgk_batch_event_times", "mgk_le_run",
            "mgk_batch_create_from", "mgk_device_memory", "mgk_correlated_field",
-           "mgk_ls_set_precision", "mgk_ls_last_solve_ms", "mgk_ls_set_wait_limit", "mgk_ls_inject_absent_cta", "mgk_ls_plan",
+           "mgk_ls_set_precision", "mgk_ls_last_solve_ms", "mgk_ls_set_wait_limit", "mgk_ls_inject_absent_cta", "mgk_ls_plan", "mgk_set_batch_plan",
            "mgk_batch_destroy"]
 
 
@@ -108,6 +108,7 @@ def lib():
     L.mgk_ls_set_wait_limit.argtypes = [vp, C.c_double]
     L.mgk_ls_inject_absent_cta.argtypes = [vp, C.c_int]
     L.mgk_ls_plan.argtypes = [vp, C.POINTER(C.c_int)]
+    L.mgk_set_batch_plan.argtypes = [C.c_int]
     L.mgk_le_run.argtypes = [C.POINTER(LeParamsC), dp, dp, dp, C.POINTER(C.c_int)]
     L.mgk_batch_event_times.argtypes = [vp, C.c_int, dp, C.c_longlong, C.POINTER(C.c_longlong)]
     L.mgk_batch_destroy.argtypes = [vp]
@@ -119,7 +120,7 @@ def lib():
                "mgk_batch_create", "mgk_batch_run", "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro",
                "mgk_batch_set_time_limit", "mgk_batch_event_times", "mgk_le_run",
                "mgk_batch_create_from", "mgk_device_memory", "mgk_correlated_field",
-               "mgk_ls_set_precision", "mgk_ls_last_solve_ms", "mgk_ls_set_wait_limit", "mgk_ls_inject_absent_cta", "mgk_ls_plan"):
+               "mgk_ls_set_precision", "mgk_ls_last_solve_ms", "mgk_ls_set_wait_limit", "mgk_ls_inject_absent_cta", "mgk_ls_plan", "mgk_set_batch_plan"):
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L

@@ -102,9 +102,12 @@ MGK_DEV void macro_from_result(const LsResult* r, BatchCtl* c, const double* w, 
         }
 }
 
-// warm-started LS solve with eps_bar = eps_macro (elastic_run) by the group
+// warm-started LS solve with eps_bar = eps_macro (elastic_run) by the group;
+// one out-of-line copy per dimension (the passes inlined in it read their
+// arguments from shared memory), shared by the replica kernels of that
+// dimension
 template <int D>
-MGK_DEV bool group_solve(BatchRep& R, int rank, const GridBar& gb, unsigned char* smem, LsArgs* sls) {
+__device__ __noinline__ bool group_solve(BatchRep& R, int rank, const GridBar& gb, unsigned char* smem, LsArgs* sls) {
     BatchCtl* c = R.ctl;
     if (threadIdx.x == 0) {
         *sls = R.ls;
@@ -974,6 +977,10 @@ __global__ void __launch_bounds__(256, 2) batch_kernel(BatchRep* reps, const int
         if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+static std::atomic<int> g_batch_plan{0};
+void set_batch_plan_objective(int objective) { g_batch_plan = objective; }
+int batch_plan_objective() { return g_batch_plan; }
+
 BatchEngine::BatchEngine(int n, const mgk_kmc_params* params, const double* const* E, const double* const* nu) {
     if (n < 1) throw std::invalid_argument("empty batch");
     // replicas are built concurrently: each one's initial catalog and barrier
@@ -1078,15 +1085,27 @@ void BatchEngine::init() {
         --ncta_[big];
         --used;
     }
+    const bool balanced = batch_plan_objective() == 1;
     while (used < budget) {
         int best = -1;
-        double gain = 0.0;
+        double key = 0.0;
         for (int r = 0; r < n; ++r) {
             if (ncta_[r] >= lim[r]) continue;
-            const double g = rate(r, ncta_[r] + 1) - rate(r, ncta_[r]);
-            if (g > gain) {
-                gain = g;
-                best = r;
+            if (balanced) {
+                // the replica furthest behind the rate it would have on the
+                // whole GPU (its modelled rate on `budget` CTAs) gets the CTA
+                const double behind = rate(r, std::min(budget, lim[r])) / rate(r, ncta_[r]);
+                if (behind > key) {
+                    key = behind;
+                    best = r;
+                }
+            } else {
+                // throughput: the replica whose modelled event rate it raises most
+                const double g = rate(r, ncta_[r] + 1) - rate(r, ncta_[r]);
+                if (g > key) {
+                    key = g;
+                    best = r;
+                }
             }
         }
         if (best < 0) break;
@@ -1100,7 +1119,12 @@ void BatchEngine::init() {
         // the LS pass plan for the replica's group, measured on the
         // replica's own grid at the group's CTA count (LsSolver::tune)
         plans[r] = eng_[r]->ls_->args_;
-        const LsPlan lp = LsSolver::autotune_enabled() ? eng_[r]->ls_->tune(ncta_[r], ls_budget) : LsPlan();
+        // measured at the largest power of two <= the group's CTA count (a
+        // serving loop re-plans its batch whenever jobs come and go: this
+        // bounds the distinct measurements per grid shape to ~9)
+        int tn = 1;
+        while (tn * 2 <= ncta_[r]) tn *= 2;
+        const LsPlan lp = LsSolver::autotune_enabled() ? eng_[r]->ls_->tune(tn, ls_budget) : LsPlan();
         const size_t need = plan_passes(plans[r], ncta_[r], ls_budget, lp);
         if (need == 0) throw std::invalid_argument("grid axis too long for the batched LS passes");
         smem_ = std::max(smem_, need);

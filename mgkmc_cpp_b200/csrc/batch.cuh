@@ -24,6 +24,15 @@ struct BatchStats {
     std::vector<double> event_us;  // device time from the previous event (or the run's first decision) to each event
 };
 
+// How a batch spreads its CTAs over the replicas (read when a batch is
+// built): 0 throughput -- each CTA to the replica whose modelled event rate
+// it raises most (small, latency-bound grids gain most); 1 balanced -- each
+// CTA to the replica whose modelled rate is furthest below its rate on the
+// whole GPU, so that every replica advances at a similar fraction of its
+// single-replica speed (a shorter makespan for mixed sizes).
+void set_batch_plan_objective(int objective);
+int batch_plan_objective();
+
 class BatchEngine {
 public:
     BatchEngine(int n, const mgk_kmc_params* params, const double* const* E, const double* const* nu);

@@ -382,6 +382,12 @@ mgk_status mgk_batch_event_times(mgk_batch* h, int replica, double* us, long lon
     return MGK_OK;
 }
 
+mgk_status mgk_set_batch_plan(int objective) {
+    if (objective < 0 || objective > 1) return fail(MGK_BAD_ARG, "batch plan: 0 throughput, 1 balanced");
+    mgk::set_batch_plan_objective(objective);
+    return MGK_OK;
+}
+
 mgk_status mgk_batch_set_time_limit(mgk_batch* h, double seconds) {
     if (!h || !(seconds > 0.0) || seconds > 3600.0) return fail(MGK_BAD_ARG, "time limit outside (0, 3600] s");
     h->b->set_time_limit(seconds);

@@ -352,7 +352,7 @@ MGK_DEV void gather_partials(const LsArgs& a, int ncta, double* out /* shared, N
 // pass layout of pass_smem).  The result goes to a.result.  Returns false
 // when a barrier wait gave up (the error word is set).
 template <int D, typename T>
-__device__ __noinline__ bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& gb, unsigned char* smem_raw) {
+MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& gb, unsigned char* smem_raw) {
     constexpr int S = D == 2 ? 3 : 6;
     constexpr int NP = 2 + 2 * S;
     __shared__ double red[14 * 32];
