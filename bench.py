@@ -354,7 +354,103 @@ def precision_block(G, cases=(((512, 512), 11), ((64, 64, 64), 12)), solves=3):
     return out
 
 
-def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05, plain_events=20):
+def kmc_precision_block(G, workloads, workdir, events=100, seed=0, workload="hetero2d_256"):
+    """The chosen form's LS re-solves in FP32-refined arithmetic against FP64:
+    the same replica (one seed of the benchmark workload) advanced `events`
+    thermal events in the batched kernel in each arithmetic, both with the
+    LS re-solves converged to a relative change of 1e-10 (the benchmark
+    description's tolerance; at the reference's 1e-6 both stop ~1e-7 from
+    the fixed point, along different paths).  Reports the
+    flip-sequence agreement (the fraction of events whose selected mode is
+    the same as in the FP64 run, up to the first difference and over the
+    whole run), the strain field's relative L2 difference after the run, the
+    device time of each and their LS iteration counts."""
+    import dataclasses
+    _, cfg = workloads.write_workload(workload, os.path.join(workdir, "prec"), seed=seed)
+    out = {}
+    res = {}
+    for prec in ("fp64", "fp32_refined"):
+        c = dataclasses.replace(cfg, ls_precision=prec, ls_tol=1e-10)
+        b = G.KmcBatch([c])
+        b.run(3)  # warm-up (its own, identical in both arithmetics up to rounding)
+        ms = b.run(events)
+        st = b.stats(0)
+        res[prec] = (st["selected"], b.field(0, "eps_field"), ms, st)
+        out[prec] = {"device_ms": ms, "events": int(st["events"]), "ls_iterations": int(st["ls_iters"]),
+                     "steps_per_s": st["events"] / (ms / 1e3) if ms > 0 else None}
+        b.close()
+    s64, e64 = res["fp64"][0], res["fp64"][1]
+    s32, e32 = res["fp32_refined"][0], res["fp32_refined"][1]
+    n = min(len(s64), len(s32))
+    same = s64[:n] == s32[:n]
+    first = int(np.argmin(same)) if not same.all() else n
+    out.update({"workload": workload, "seed": seed, "events_compared": n, "identical_prefix": first,
+                "flip_agreement": float(same.mean()) if n else None,
+                "field_rel_l2_vs_fp64": float(np.linalg.norm(e32 - e64) / np.linalg.norm(e64)),
+                "speedup": out["fp64"]["device_ms"] / out["fp32_refined"]["device_ms"]
+                if out["fp32_refined"]["device_ms"] > 0 else None})
+    progress("kmc precision: agreement %s, field %.2e, speedup %.2f" % (out["flip_agreement"],
+                                                                          out["field_rel_l2_vs_fp64"], out["speedup"]))
+    return out
+
+
+def cfg2_block(G, workloads, workdir, events=10):
+    """The benchmark's config 2 physics (workload bl_cfg2_64: 3D 64^3, lognormal
+    E CoV 0.15, 100 Fibonacci-plane shears of gamma0 0.1 along the local
+    resolved shear stress, per-voxel dF N(1.0, 0.1) eV clipped to [0.6, 1.4],
+    z tension): thermal events per second of the plain and the batched form."""
+    _, cfg = workloads.write_workload("bl_cfg2_64", os.path.join(workdir, "cfg2"), seed=0)
+    kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
+    sim = G.from_config(cfg, output_dir=None)
+    sim.run_simulation(10 ** 6, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50, max_events=2, **kw)
+    sim.set_profiling(True)
+    e0 = sim.stats["thermal_events"]
+    sim.run_simulation(10 ** 6, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50, max_events=events, **kw)
+    ev = sim.stats["thermal_events"] - e0
+    plain = ev / (sim.profile()["run_ms"] / 1e3) if ev else None
+    del sim
+    b = G.KmcBatch([cfg])
+    b.run(2)
+    ms = b.run(events)
+    st = b.stats(0)
+    b.close()
+    out = {"workload": "bl_cfg2_64", "modes": cfg.n_voxels * cfg.M, "plain_steps_per_s": plain,
+           "batched_steps_per_s": st["events"] / (ms / 1e3) if ms > 0 else None, "batched_events": int(st["events"]),
+           "ls_iterations_per_step": st["ls_iters"] / max(st["events"], 1)}
+    progress("cfg2: plain %s, batched %s steps/s" % (plain, out["batched_steps_per_s"]))
+    return out
+
+
+def ls_sweep_block(G, grids, iters=20, reps=5):
+    """The FP64 LS iteration alone: for each grid (a seeded lognormal modulus
+    field, CoV 0.1), cold solves of 2 and 2 + iters fixed iterations (tol 0),
+    the difference of their median device times over `iters`; algorithmic
+    bytes 136 B (2D) / 256 B (3D) per voxel-iteration; the measured pass plan."""
+    from mgkmc_cpp_b200 import fields
+    out = {}
+    for dims in grids:
+        D, N = len(dims), int(np.prod(dims))
+        E = fields.lognormal_modulus(dims, 90e9, 0.10, 4.0 if D == 2 else 3.0, 3).reshape(-1)
+        s = G.LsSolver(dims, E, np.full(N, 0.36))
+        eb = np.zeros((D, D))
+        eb[0, 0], eb[1, 1] = 1e-3, -4e-4
+        s.solve(eb, max_iter=5, tol=0.0)
+        t = {}
+        for it in (2, 2 + iters):
+            ms = []
+            for _ in range(reps):
+                s.solve(eb, max_iter=it, tol=0.0)
+                ms.append(s.last_solve_ms())
+            t[it] = float(np.median(ms))
+        per = (t[2 + iters] - t[2]) / iters
+        row = {"us_per_iteration": per * 1e3, "achieved_gbs": BYTES_LS[D] * N / (per * 1e-3) / 1e9, "plan": s.plan()}
+        s.close()
+        out["x".join(map(str, dims))] = row
+        progress("ls: %s %.2f us/iteration" % (dims, per * 1e3))
+    return out
+
+
+def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05, plain_events=20, max_seconds=None):
     """The serving loop on a Poisson request stream (20 jobs/s, seed 7): jobs
     are admitted as they arrive (wall clock) and as memory allows, every
     active job advances in shared batched launches of slice_seconds of device
@@ -366,8 +462,12 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05,
         srv.submit(cfg, target, arrival=arrival)
     t0 = time.perf_counter()
     dev_ms = 0.0
+    capped = False
     while not srv.idle():
         now = time.perf_counter() - t0
+        if max_seconds is not None and now > max_seconds:
+            capped = True  # the window ends: report what finished and what ran
+            break
         if not srv.active and srv.queue and srv.queue[0]["arrival"] > now:
             time.sleep(min(0.05, srv.queue[0]["arrival"] - now))
             continue
@@ -377,6 +477,7 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05,
                                                                                 len(srv.queue), len(srv.done)))
     wall = time.perf_counter() - t0
     done = list(srv.done.values())
+    events_unfinished = sum(j["events"] for j in srv.active)
     events = sum(j["events"] for j in done)
     stalled = [j for j in done if j["stalled"]]
     terminated = [j for j in done if not j["stalled"] and j["events"] < j["target"]]
@@ -400,17 +501,21 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05,
         ev = sim.stats["thermal_events"] - e0
         rates[key] = ev / (sim.profile()["run_ms"] / 1e3) if ev else 0.0
         del sim
-    plain_s = sum(j["events"] / rates[(j["cfg"].dim, j["cfg"].nx)] for j in done
+    served = done + list(srv.active)
+    plain_s = sum(j["events"] / rates[(j["cfg"].dim, j["cfg"].nx)] for j in served
                   if rates.get((j["cfg"].dim, j["cfg"].nx)))
+    ev_all = events + events_unfinished
     return {"jobs": len(done), "arrivals": "Poisson 20 jobs/s, seed 7", "flips_per_job": list(flips),
             "sizes": ["%s %d" % x for x in sizes], "slice_seconds": slice_seconds, "events": int(events),
             "wall_seconds": wall, "device_seconds": dev_ms / 1e3, "launches": srv.launches,
             "stalled_jobs": len(stalled), "stalled_why": "no thermal event for %.0f s of device time (an avalanche "
                                                         "whose cascade batches never settle)" % srv.stall_seconds,
             "terminated_jobs": len(terminated),
-            "value": events / wall if wall > 0 else None, "unit": UNIT,
-            "plain_job_by_job_seconds": plain_s, "plain_steps_per_s": events / plain_s if plain_s > 0 else None,
-            "speedup_vs_plain": (events / wall) / (events / plain_s) if plain_s > 0 and wall > 0 else None,
+            "value": (events + events_unfinished) / wall if wall > 0 else None, "unit": UNIT,
+            "window_capped": capped, "jobs_unfinished": len(srv.active) + len(srv.queue),
+            "events_in_unfinished_jobs": int(events_unfinished),
+            "plain_job_by_job_seconds": plain_s, "plain_steps_per_s": ev_all / plain_s if plain_s > 0 else None,
+            "speedup_vs_plain": plain_s / wall if plain_s > 0 and wall > 0 else None,
             "plain_rates_by_class": {"%dD %d" % k: v for k, v in rates.items()},
             "step_latency_us": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},
             "job_completion_s": {"p50": percentile(comp, 50), "p99": percentile(comp, 99)}}
@@ -428,6 +533,8 @@ def main():
     ap.add_argument("--ref-events", type=int, default=150, help="events per replica timed by --impl reference")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-replica ensemble block")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP64 / FP32-refined LS block")
+    ap.add_argument("--ls-sweep", nargs="+", default=None, metavar="NXxNY[xNZ]",
+                    help="run only the FP64 LS iteration microbenchmark on these grids and print its JSON")
     ap.add_argument("--only-precision", action="store_true",
                     help="run only the FP64 / FP32-refined LS block and print its JSON (profiling the LS kernels)")
     ap.add_argument("--ensemble-seconds", type=float, default=40.0)
@@ -435,6 +542,8 @@ def main():
                     help="how the ensemble's batch spreads CTAs over the replicas (mgk_set_batch_plan)")
     ap.add_argument("--serve-jobs", type=int, default=40, help="jobs of the serving block (0: skip)")
     ap.add_argument("--serve-flips", type=int, nargs=2, default=[50, 500])
+    ap.add_argument("--serve-seconds", type=float, default=None, help="wall-time cap of the serving block")
+    ap.add_argument("--serve-plan", default="throughput", choices=["throughput", "balanced"])
     ap.add_argument("--serve-full-sizes", action="store_true",
                     help="serve the full size set (2D 32^2..512^2, 3D 32^3, 64^3); default 2D 32^2..256^2, 3D 32^3")
     args = ap.parse_args()
@@ -487,6 +596,10 @@ def main():
 
     if args.only_precision:
         print(json.dumps({"precision": precision_block(G)}))
+        return 0
+    if args.ls_sweep:
+        grids = [tuple(int(x) for x in g.lower().split("x")) for g in args.ls_sweep]
+        print(json.dumps({"ls_sweep": ls_sweep_block(G, grids)}))
         return 0
 
     dist, dev = None, None
@@ -584,12 +697,20 @@ def main():
             G.set_batch_plan("throughput")
         except Exception as e:  # reported, never silently dropped
             ens = {"error": str(e)[-300:]}
-    prec = None
+    prec = kprec = c2 = None
     if rank == 0 and not args.no_precision:
         try:
             prec = precision_block(G)
         except Exception as e:
             prec = {"error": str(e)[-300:]}
+        try:
+            kprec = kmc_precision_block(G, workloads, workdir)
+        except Exception as e:
+            kprec = {"error": str(e)[-300:]}
+        try:
+            c2 = cfg2_block(G, workloads, workdir)
+        except Exception as e:
+            c2 = {"error": str(e)[-300:]}
     srv = None
     progress("serving")
     if args.serve_jobs > 0 and rank == 0:
@@ -597,7 +718,11 @@ def main():
                                                                      if x in (("2d", 32), ("2d", 64), ("2d", 128),
                                                                               ("2d", 256), ("3d", 32))]
         try:
-            srv = serve_block(G, workloads, workdir, args.serve_jobs, tuple(args.serve_flips), sizes)
+            G.set_batch_plan(args.serve_plan)
+            srv = serve_block(G, workloads, workdir, args.serve_jobs, tuple(args.serve_flips), sizes,
+                              max_seconds=args.serve_seconds)
+            srv["plan"] = args.serve_plan
+            G.set_batch_plan("throughput")
         except Exception as e:
             srv = {"error": str(e)[-300:]}
     if rank != 0:
@@ -650,6 +775,10 @@ def main():
         line["serving"] = srv
     if prec is not None:
         line["precision"] = prec
+    if kprec is not None:
+        line["kmc_precision"] = kprec
+    if c2 is not None:
+        line["cfg2"] = c2
     if args.gpus == 1:
         progress("cpu baseline")
         res, err = run_reference(cfg_paths, args.cpu_events)

@@ -60,3 +60,34 @@ def test_fp32_refined_against_reference_golden():
     d32 = rel(res["fp32_refined"][0], g["eps"])
     assert d64 < 1e-10
     assert d32 < 1e-6
+
+
+@pytest.mark.parametrize("workload", ["hetero2d_64", "hetero3d_16"])
+def test_kmc_fp32_refined_flips_and_fields_match_fp64(workload, tmp_path):
+    """The chosen arithmetic in both KMC forms: every re-solve FP32-refined
+    (ls.precision fp32_refined) against the FP64 run (which the reference
+    pins), both converged to 1e-10: the same flips, fields within 1e-8."""
+    import dataclasses
+    import mgkmc_cpp_b200 as G
+    from mgkmc_cpp_b200 import workloads
+    G._lib.require_device()
+    _, cfg = workloads.write_workload(workload, str(tmp_path), seed=2)
+    nev = 120 if cfg.dim == 2 else 40
+    runs = {}
+    for prec in ("fp64", "fp32_refined"):
+        c = dataclasses.replace(cfg, ls_precision=prec, ls_tol=1e-10)
+        sim = G.from_config(c, output_dir=str(tmp_path))
+        tr = sim.run_simulation(10 ** 6, c.step_size, c.driving, c.targets, c.mixed_tol_pa, 50,
+                                enable_console_log=False, enable_summary_log=False, enable_global_log=False,
+                                max_events=nev, trace=True)
+        b = G.KmcBatch([c])
+        b.run(nev)
+        runs[prec] = (tr[tr[:, 0] == 0, 1].astype(np.int64), sim.eps_field, b.stats(0)["selected"],
+                      b.field(0, "eps_field"))
+        b.close()
+    sel64, eps64, bsel64, beps64 = runs["fp64"]
+    sel32, eps32, bsel32, beps32 = runs["fp32_refined"]
+    assert len(sel64) == nev and np.array_equal(sel32, sel64)
+    assert np.array_equal(bsel32, sel64) and np.array_equal(bsel64, sel64)
+    assert rel(eps32, eps64) < 1e-8
+    assert rel(beps32, eps64) < 1e-8
