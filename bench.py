@@ -484,13 +484,15 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05,
     comp = [j["finished"] - j["arrival"] for j in done]
     lat = np.array(srv.step_latency_us)
     # the plain form on the same job stream: each size class's rate on its
-    # first job (plain_events events after 3 of warm-up), every job's events
-    # at its class's rate, one job after another
+    # first job that reached its target (plain_events events after 3 of
+    # warm-up; a stalled job's avalanche would never end a plain run), every
+    # job's events at its class's rate, one job after another
     kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
     rates = {}
-    for _, cfg, _ in jobs:
+    for j in sorted(done, key=lambda x: x["id"]):
+        cfg = j["cfg"]
         key = (cfg.dim, cfg.nx)
-        if key in rates:
+        if key in rates or j["stalled"] or j["events"] < plain_events + 3:
             continue
         sim = G.from_config(cfg, output_dir=None)
         sim.run_simulation(10 ** 6, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50, max_events=3, **kw)
@@ -697,6 +699,7 @@ def main():
             G.set_batch_plan("throughput")
         except Exception as e:  # reported, never silently dropped
             ens = {"error": str(e)[-300:]}
+            progress("ensemble failed: " + ens["error"])
     prec = kprec = c2 = None
     if rank == 0 and not args.no_precision:
         try:
@@ -707,10 +710,12 @@ def main():
             kprec = kmc_precision_block(G, workloads, workdir)
         except Exception as e:
             kprec = {"error": str(e)[-300:]}
+            progress("kmc precision failed: " + kprec["error"])
         try:
             c2 = cfg2_block(G, workloads, workdir)
         except Exception as e:
             c2 = {"error": str(e)[-300:]}
+            progress("cfg2 failed: " + c2["error"])
     srv = None
     progress("serving")
     if args.serve_jobs > 0 and rank == 0:
@@ -725,6 +730,7 @@ def main():
             G.set_batch_plan("throughput")
         except Exception as e:
             srv = {"error": str(e)[-300:]}
+            progress("serving failed: " + srv["error"])
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
