@@ -172,7 +172,7 @@ size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, LsPlan plan) {
     const size_t tw_b = al(maxn * elem);
     auto row_b = [&](int r) { return (size_t)((r * S + 1) / 2) * padded_len(a.nr) * elem; };
     auto col_b = [&](int t) { return (size_t)S * t * colp * elem; };
-    auto total = [&](size_t line) { return (two ? 2 : 1) * al(line) + tw_b; };
+    auto total = [&](size_t line) { return (two ? 2 : 1) * al(line) + tw_b + kLsScratchBytes; };
     if (total(std::max(row_b(1), col_b(1))) > smem_cap) return 0;
     // largest chunk / tile that fits
     int rpb_max = 1;
@@ -194,7 +194,8 @@ size_t plan_passes(LsArgs& a, int ncta, size_t smem_cap, LsPlan plan) {
     const size_t line = al(std::max(row_b(a.rpb), col_b(a.tk)));
     a.smem_half = (int)line;
     a.tw_off = (int)((two ? 2 : 1) * line);
-    return (size_t)a.tw_off + tw_b;
+    a.scr_off = a.tw_off + (int)tw_b;
+    return (size_t)a.scr_off + kLsScratchBytes;
 }
 
 static void lame(double E, double nu, int D, bool ps, double* lam, double* mu) {

@@ -30,6 +30,11 @@ constexpr int kMaxPartials = 16;
 // such CTAs and their static shared memory fit an SM's 228 KB).
 constexpr int kLsCtasPerSm = 2;
 constexpr size_t kLsSmemCap = 104 * 1024;
+// Reduction scratch of a solve in its dynamic shared memory: block sums (14
+// values x 32 warps), the 256 group sums of the partials' gather, the sums
+// and the warm-start shift.  (As static arrays every template instance of
+// the solve held its own copy: 23 KB of the batched kernel's shared memory.)
+constexpr size_t kLsScratchBytes = sizeof(double) * (14 * 32 + 256 + 16 + 8);
 // relative-change target of the FP32 phase of an FP32-refined solve: above
 // the FP32 rounding floor of the iteration (~1e-7 relative)
 constexpr double kFp32Tol = 1e-6;
@@ -58,6 +63,7 @@ struct LsArgs {
     double diff_extra_first;  // antisymmetric part of |eps_new - eps|^2 in the first iteration
     int smem_half;         // byte offset of the second line buffer
     int tw_off;            // byte offset of the shared-memory twiddle table
+    int scr_off;           // byte offset of the reduction scratch (kLsScratchBytes)
     double ebar_s[6];      // symmetric part of the prescribed mean strain
     double lam0, mu0, inv2mu0, bcoef;
     double pixel;

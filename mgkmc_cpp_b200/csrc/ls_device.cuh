@@ -329,8 +329,7 @@ MGK_DEV void publish_partials(const LsArgs& a, int cta, double* part, double* re
 // once, in the last CTA to reach the barrier, and reading the sums back was
 // measured slower: one more L2 round trip on the critical path.)
 template <int NP>
-MGK_DEV void gather_partials(const LsArgs& a, int ncta, double* out /* shared, NP */) {
-    __shared__ double grp[256];
+MGK_DEV void gather_partials(const LsArgs& a, int ncta, double* out /* shared, NP */, double* grp /* shared, 256 */) {
     const int k = threadIdx.x & 15, g = threadIdx.x >> 4;
     double s = 0.0;
     if (k < NP) {
@@ -355,9 +354,10 @@ template <int D, typename T>
 MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& gb, unsigned char* smem_raw) {
     constexpr int S = D == 2 ? 3 : 6;
     constexpr int NP = 2 + 2 * S;
-    __shared__ double red[14 * 32];
-    __shared__ double vals[14];
-    __shared__ double s_shift[6];
+    double* red = reinterpret_cast<double*>(smem_raw + a.scr_off);  // 14 x 32
+    double* grp = red + 14 * 32;                                    // 256
+    double* vals = grp + 256;                                       // 16
+    double* s_shift = vals + 16;                                    // 8
     // fault injection (set from the host for tests): this CTA never arrives,
     // so the others' bounded waits run out and they return with the error set
     if (a.test_absent == cta + 1) return false;
@@ -376,7 +376,7 @@ MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& g
         }
         publish_partials<NP>(a, cta, acc, red);
         if (!grid_sync(gb)) return false;
-        gather_partials<NP>(a, ncta, vals);
+        gather_partials<NP>(a, ncta, vals, grp);
         if (threadIdx.x < S) s_shift[threadIdx.x] = a.ebar_s[threadIdx.x] - vals[threadIdx.x] * a.inv_n;
         __syncthreads();
 #pragma unroll
@@ -390,7 +390,7 @@ MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& g
     row_pass<D, T, 0>(a, cta, ncta, smem_raw, part, shift);
     publish_partials<NP>(a, cta, part, red);
     if (!grid_sync(gb)) return false;
-        gather_partials<NP>(a, ncta, vals);
+        gather_partials<NP>(a, ncta, vals, grp);
     int it = 0;
     double diff = 0.0;
     while (it < a.max_iter) {
@@ -409,7 +409,7 @@ MGK_DEV bool ls_solve_group(const LsArgs& a, int cta, int ncta, const GridBar& g
         row_pass<D, T, 1>(a, cta, ncta, smem_raw, part, shift);
         publish_partials<NP>(a, cta, part, red);
         if (!grid_sync(gb)) return false;
-        gather_partials<NP>(a, ncta, vals);
+        gather_partials<NP>(a, ncta, vals, grp);
         const double dx = it == 0 ? a.diff_extra_first : 0.0;
         const double nx = it == 0 ? a.norm_extra_first : a.norm_extra;
         ++it;
