@@ -41,7 +41,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import subprocess
 import sys
 import tempfile
@@ -125,25 +124,32 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def traffic_from_profiles(workload: str):
-    """DRAM bytes per LS launch from the committed ncu summary, if present."""
-    p = os.path.join(HERE, "profiles", "ls_kernel_%s.md" % workload)
+def _traffic(key: str):
+    """A DRAM-traffic figure (dram__bytes_read.sum + dram__bytes_write.sum of
+    one ncu capture, scaled to the unit named by the key) from
+    profiles/traffic.json, written beside the ncu summaries it comes from."""
+    p = os.path.join(HERE, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+    with open(p) as f:
+        return json.load(f).get(key)
+
+
+def traffic_from_profiles(workload: str, iterations_per_launch: float):
+    """DRAM bytes of one plain-form LS launch: the captured launch's bytes per
+    LS iteration (ncu, ls_kernel on the workload's grid) times the launches'
+    mean iteration count."""
+    t = _traffic("ls_kernel/%s/bytes_per_iteration" % workload)
+    return t * iterations_per_launch if t is not None else None
 
 
 def batch_traffic_from_profiles(workload: str, events: float):
     """DRAM bytes of a batch_kernel launch of `events` thermal events: the
-    committed ncu summary's bytes per event (a 4-replica, 20-event capture)
-    times the events, traffic growing with the events (each is a sweep and its
-    LS iterations).  None without the summary."""
-    p = os.path.join(HERE, "profiles", "batch_kernel_%sx4.md" % workload)
-    if not os.path.exists(p):
-        return None
-    m = re.search(r"traffic_bytes_per_event:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) * events if m else None
+    captured launch's bytes per thermal event (the same four replicas) times
+    the events, traffic growing with the events (each is a sweep and its LS
+    iterations).  None without the figure."""
+    t = _traffic("batch_kernel/%sx4/bytes_per_event" % workload)
+    return t * events if t is not None else None
 
 
 def host_cpu():
@@ -758,7 +764,8 @@ def main():
                                    "redraws and LS solves)", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": batch_traffic_from_profiles(args.workload, ev),
-                         "traffic_note": "ncu DRAM bytes per event of a 20-event capture, times the launch's events",
+                         "traffic_note": "ncu DRAM bytes per thermal event of a captured launch of the same four "
+                                         "replicas (profiles/traffic.json), times this launch's events",
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / max(ev2, 1),
                     "d2h_bytes_per_step": d2h / max(ev2, 1)},
@@ -772,7 +779,9 @@ def main():
                       "gpu_launches": int(p1["launches"] - p0["launches"]),
                       "roofline": {"kernel": "ls_kernel (one persistent launch per LS solve)", "bound": "hbm",
                                    "achieved": ls_achieved, "peak": peak, "unit": "GB/s", "frac": ls_achieved / peak,
-                                   "traffic": traffic_from_profiles(args.workload), "alg_bytes_per_launch": ls_bytes,
+                                   "traffic": traffic_from_profiles(args.workload,
+                                                                    prof["ls_iterations"] / n_launch),
+                                   "alg_bytes_per_launch": ls_bytes,
                                    "avg_launch_ms": avg_ms}},
             "clocks": clk}
     if ens is not None:

@@ -26,13 +26,15 @@ def test_reference_arm_json_line():
 
 
 def test_roofline_traffic_from_committed_profiles():
-    """The roofline's DRAM traffic comes from the committed ncu summaries: the
-    LS kernel's bytes per launch, and the batch kernel's bytes per event scaled
-    by the events of the timed launch."""
+    """The roofline's DRAM traffic comes from profiles/traffic.json, beside the
+    committed ncu summaries: the LS kernel's bytes per iteration scaled by a
+    launch's iterations, and the batch kernel's bytes per event scaled by the
+    events of the timed launch."""
     sys.path.insert(0, ROOT)
     import bench
-    ls = bench.traffic_from_profiles("hetero2d_256")
+    ls = bench.traffic_from_profiles("hetero2d_256", 10.0)
     assert ls is not None and ls > 0
+    assert bench.traffic_from_profiles("hetero2d_256", 20.0) == 2 * ls
     per_event = bench.batch_traffic_from_profiles("hetero2d_256", 1)
     assert per_event is not None and 1e6 < per_event < 1e9
     assert bench.batch_traffic_from_profiles("hetero2d_256", 4000) == 4000 * per_event
