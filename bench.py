@@ -255,7 +255,7 @@ def ensemble_block(G, workloads, workdir, seconds, plain_events):
     b.set_time_limit(min(seconds, 5.0))
     b.run(10 ** 9)  # warm-up
     progress("ensemble: warm-up done")
-    # timed: every replica stops at its first decision past the window; the
+    # timed: once every replica is past the window each stops at its next decision; the
     # launch ends when the last one does (its overshoot is counted as time)
     b.set_time_limit(seconds)
     ms = b.run(10 ** 9)

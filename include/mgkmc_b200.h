@@ -268,10 +268,13 @@ MGK_API mgk_status mgk_le_run(const mgk_le_params* p, const double* E, const dou
  * interval ends (mixed-BC loop), then the number of sweeps and the bytes the
  * run call copied host-to-device and device-to-host for the replica} and
  * copies the flat mode index of each thermal event of the last run into sel
- * (up to sel_cap; *sel_len gets the count).  A run stops every replica whose
- * run call has lasted longer than the time limit (default 60 s, set with
- * mgk_batch_set_time_limit) at its next decision and returns MGK_TIME_LIMIT;
- * the state stays consistent and a later run continues from it. */
+ * (up to sel_cap; *sel_len gets the count).  Time limit (default 60 s, set
+ * with mgk_batch_set_time_limit): a replica whose run call has lasted longer
+ * keeps working until every replica of the batch has (or has finished), then
+ * every replica stops at its next decision -- the launch waits for its
+ * slowest replica's decision in any case, so the others use that time -- and
+ * the call returns MGK_TIME_LIMIT; the state stays consistent and a later
+ * run continues from it. */
 typedef struct mgk_batch mgk_batch;
 MGK_API mgk_status mgk_batch_create(mgk_batch** out, int n, const mgk_kmc_params* params, const double* const* E,
                                     const double* const* nu);

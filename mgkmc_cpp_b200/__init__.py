@@ -658,7 +658,8 @@ class KmcBatch:
         self._h = h
 
     def set_time_limit(self, seconds: float):
-        """Wall-time bound of one run call (default 60 s)."""
+        """Wall-time bound of one run call (default 60 s): once every replica
+        has run past it (or finished), each stops at its next decision."""
         _lib.check(_lib.lib().mgk_batch_set_time_limit(self._h, float(seconds)))
 
     def run(self, max_events: int, n_global_steps=10 ** 6, max_cascade_batches=0, budgets=None) -> float:

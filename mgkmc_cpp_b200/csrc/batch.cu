@@ -54,6 +54,7 @@ struct BatchCtl {
     long long events_total, cascades, cascade_flips, ls_solves, ls_iters, elastic_steps, fallbacks, sweeps;
     int sel_log_len, sel_log_cap;
     unsigned long long t_start_ns, limit_ns;  // device clock at the first decision; 0: unset
+    int past_marked, pad_pm;                  // counted in the batch's past-the-limit word
     unsigned long long ph_ns[6];              // sweep, decide, event solve, cascade flips, cascade solve, interval end
 };
 
@@ -80,6 +81,7 @@ struct BatchRep {
     BatchCtl* ctl;
     int* sel_log;
     unsigned long long* ev_ns;  // device clock at the end of each logged thermal event
+    unsigned* past;  // batch-wide: {replicas past the time limit or finished, replicas}
 };
 
 namespace {
@@ -532,8 +534,21 @@ MGK_DEV int decide(BatchRep& R, rng::MtRing* ring, rng::Mt* g, unsigned char* sm
         double target = 0.0;
         const unsigned long long now = global_ns();
         if (c->t_start_ns == 0) c->t_start_ns = now;
+        // time limit of one run call (a sustained avalanche never ends an
+        // event): a replica past it keeps working until every replica of the
+        // batch is past it (or finished), then stops at its next decision --
+        // the launch lasts until its slowest replica's decision anyway, and
+        // the others stay busy meanwhile
+        bool stop = false;
         if (now - c->t_start_ns > c->limit_ns) {
-            act = ACT_STOP;  // wall-time bound of one run call (a sustained avalanche never ends)
+            if (!c->past_marked) {
+                c->past_marked = 1;
+                atomicAdd(R.past, 1u);
+            }
+            stop = *(volatile unsigned*)R.past >= R.past[1];
+        }
+        if (stop) {
+            act = ACT_STOP;
             c->status = 2;
             c->done = 1;
         } else if (!R.p.kmc_mode && nun > 0) {
@@ -951,6 +966,10 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
         }
         if (!grid_sync(gb)) break;
     }
+    if (rank == 0 && threadIdx.x == 0 && !c->past_marked) {  // finished (or failed): no longer holds the others
+        c->past_marked = 1;
+        atomicAdd(R.past, 1u);
+    }
     if (rank == 0) {
         __syncthreads();
         rng::ring_store(&s_ring, &s_mt);
@@ -1182,6 +1201,8 @@ void BatchEngine::init() {
         BCK(cudaMemset(R.bar, 0, 4 * sizeof(unsigned)));
         for (int k = 0; k < R.ncta; ++k) map.push_back(make_int2(r, k));
     }
+    BCK(cudaMalloc((void**)&d_past_, 2 * sizeof(unsigned)));
+    for (auto& R : reps) R.past = d_past_;
     alloc_reps_ = nullptr;
     BCK(cudaMalloc((void**)&alloc_reps_, sizeof(BatchRep) * n));
     BCK(cudaMemcpy(alloc_reps_, reps.data(), sizeof(BatchRep) * n, cudaMemcpyHostToDevice));
@@ -1196,6 +1217,7 @@ BatchEngine::~BatchEngine() {
     for (void* p : owned_) cudaFree(p);
     cudaFree(alloc_reps_);
     cudaFree(map_);
+    cudaFree(d_past_);
     eng_.clear();
     owned_eng_.clear();
     if (st_) cudaStreamDestroy(st_);
@@ -1274,6 +1296,8 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             BCK(cudaMemsetAsync(reps_host_[r].bar, 0, 4 * sizeof(unsigned), st_));
             BCK(cudaStreamSynchronize(st_));
         }
+        const unsigned past0[2] = {0u, (unsigned)n};
+        BCK(cudaMemcpyAsync(d_past_, past0, sizeof(past0), cudaMemcpyHostToDevice, st_));
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);

@@ -62,6 +62,7 @@ private:
     std::vector<BatchStats> last_;
     BatchRep* alloc_reps_ = nullptr;
     int2* map_ = nullptr;
+    unsigned* d_past_ = nullptr;  // {replicas past the time limit or finished, replicas}
     size_t smem_ = 0;
     int total_ctas_ = 0;
     double time_limit_s_ = 60.0;
