@@ -629,10 +629,11 @@ def main():
 
     # chosen form: all replicas in one device-resident launch
     progress("chosen form: %d replicas" % len(cfgs))
-    batch = G.KmcBatch(cfgs)
-    # clocks sampled from the warm-up to the end of the plain form's timed run
+    # clocks sampled from before the batch is built (nvidia-smi takes ~0.5 s to
+    # start) to the end of the plain form's timed run
     clocks = ClockSampler(local_rank)
     clocks.start()
+    batch = G.KmcBatch(cfgs)
     batch.run(args.warmup)
     barrier()
     # one public call: its launch is timed on the device (value) and the
