@@ -463,7 +463,9 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05,
     time, finished jobs retire.  Returns throughput, per-step latency and job
     completion latency."""
     jobs = workloads.serve_jobs(os.path.join(workdir, "serve"), n_jobs, flips=flips, sizes=sizes)
-    srv = G.Server(slice_seconds=slice_seconds)
+    # a job without a thermal event for 5 s of device time is in an avalanche
+    # that never ends (the reference would run it forever): retired as stalled
+    srv = G.Server(slice_seconds=slice_seconds, stall_seconds=5.0)
     for arrival, cfg, target in jobs:
         srv.submit(cfg, target, arrival=arrival)
     t0 = time.perf_counter()

@@ -62,17 +62,19 @@ def test_fp32_refined_against_reference_golden():
     assert d32 < 1e-6
 
 
-@pytest.mark.parametrize("workload", ["hetero2d_64", "hetero3d_16"])
+@pytest.mark.parametrize("workload", ["ens2d_64", "ens3d_32"])
 def test_kmc_fp32_refined_flips_and_fields_match_fp64(workload, tmp_path):
     """The chosen arithmetic in both KMC forms: every re-solve FP32-refined
     (ls.precision fp32_refined) against the FP64 run (which the reference
-    pins), both converged to 1e-10: the same flips, fields within 1e-8."""
+    pins), both converged to 1e-10: the same flips, fields within 1e-8.
+    (Workloads with the reference's default barriers: the N(1.0, 0.1) ones can
+    enter avalanches that never end a plain-form run.)"""
     import dataclasses
     import mgkmc_cpp_b200 as G
     from mgkmc_cpp_b200 import workloads
     G._lib.require_device()
     _, cfg = workloads.write_workload(workload, str(tmp_path), seed=2)
-    nev = 120 if cfg.dim == 2 else 40
+    nev = 120 if cfg.dim == 2 else 30
     runs = {}
     for prec in ("fp64", "fp32_refined"):
         c = dataclasses.replace(cfg, ls_precision=prec, ls_tol=1e-10)
