@@ -456,7 +456,8 @@ def ls_sweep_block(G, grids, iters=20, reps=5):
     return out
 
 
-def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05, plain_events=20, max_seconds=None):
+def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05, plain_events=20, max_seconds=None,
+                build_threads=4):
     """The serving loop on a Poisson request stream (20 jobs/s, seed 7): jobs
     are admitted as they arrive (wall clock) and as memory allows, every
     active job advances in shared batched launches of slice_seconds of device
@@ -465,7 +466,10 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05,
     jobs = workloads.serve_jobs(os.path.join(workdir, "serve"), n_jobs, flips=flips, sizes=sizes)
     # a job without a thermal event for 5 s of device time is in an avalanche
     # that never ends (the reference would run it forever): retired as stalled
-    srv = G.Server(slice_seconds=slice_seconds, stall_seconds=5.0)
+    # jobs after the first of their grid shape are built on host threads
+    # while the GPU runs the active ones (their initial draws follow the
+    # reference's sequential random stream on the host)
+    srv = G.Server(slice_seconds=slice_seconds, stall_seconds=5.0, build_threads=build_threads)
     for arrival, cfg, target in jobs:
         srv.submit(cfg, target, arrival=arrival)
     t0 = time.perf_counter()
@@ -484,6 +488,7 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05,
             progress("serving: %d launches, %d active, %d queued, %d done" % (srv.launches, len(srv.active),
                                                                                 len(srv.queue), len(srv.done)))
     wall = time.perf_counter() - t0
+    srv.close()
     done = list(srv.done.values())
     events_unfinished = sum(j["events"] for j in srv.active)
     events = sum(j["events"] for j in done)
@@ -518,6 +523,8 @@ def serve_block(G, workloads, workdir, n_jobs, flips, sizes, slice_seconds=0.05,
     return {"jobs": len(done), "arrivals": "Poisson 20 jobs/s, seed 7", "flips_per_job": list(flips),
             "sizes": ["%s %d" % x for x in sizes], "slice_seconds": slice_seconds, "events": int(events),
             "wall_seconds": wall, "device_seconds": dev_ms / 1e3, "launches": srv.launches,
+            "build_threads": build_threads, "jobs_built_on_threads": srv.built_on_pool,
+            "host_seconds": {k: round(v, 2) for k, v in srv.host_seconds.items()},
             "stalled_jobs": len(stalled), "stalled_why": "no thermal event for %.0f s of device time (an avalanche "
                                                         "whose cascade batches never settle)" % srv.stall_seconds,
             "terminated_jobs": len(terminated),

@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import dataclasses
 import os
+import time
 from typing import Dict, Optional, Tuple
 
 import numpy as np
@@ -461,6 +462,10 @@ def job_device_bytes(cfg) -> int:
     return int(N * cfg.M * 8 * (2 + C) + N * 8 * (4 * S + 2 + 2 + 2 * S + 2 + 1 + C) + (64 << 10))
 
 
+def _shape_key(cfg):
+    return (cfg.dim, cfg.nx, cfg.ny, cfg.nz if cfg.dim == 3 else 1, cfg.plane_mode)
+
+
 class Server:
     """Continuous batching of KMC jobs on one GPU (the serving loop).
 
@@ -476,10 +481,17 @@ class Server:
     ``slice_events`` events each, when given) and retires the jobs that
     reached their target (or made no progress for ``stall_seconds``).  A job's trajectory does not depend on
     what shares its launches: its random stream and interval clock are its
-    own."""
+    own.
+
+    With ``build_threads`` > 0 an admitted job's simulation is built on a
+    thread pool while the active jobs keep running (its initial catalog and
+    barriers are drawn on the host from the reference's sequential random
+    stream: seconds for a large 3D grid); it joins the batch at the first
+    step after its build finished.  Its memory counts against the budget from
+    admission."""
 
     def __init__(self, max_active=64, slice_events=None, slice_seconds=0.05, reserve_bytes=8 << 30, hbm_budget=None,
-                 stall_seconds=30.0):
+                 stall_seconds=30.0, build_threads=0):
         self.max_active, self.reserve = int(max_active), int(reserve_bytes)
         self.slice_events = None if slice_events is None else int(slice_events)
         self.slice_seconds = float(slice_seconds)
@@ -488,9 +500,17 @@ class Server:
         self.stall_seconds = float(stall_seconds)
         self._batch, self._batch_ids = None, None
         self.queue, self.active, self.done = [], [], {}
+        self.building = []  # admitted jobs whose simulation is being built
+        self._shapes = set()  # grid shapes built so far
+        self.built_on_pool = 0
+        self._pool = None
+        if int(build_threads) > 0:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(int(build_threads), thread_name_prefix="mgk-build")
         self._next = 0
         self.launches = 0
         self.step_latency_us = []
+        self.host_seconds = {"build_wait": 0.0, "rebuild": 0.0, "readback": 0.0, "retire": 0.0}
 
     def submit(self, cfg, flips: int, arrival: float = 0.0) -> int:
         jid = self._next
@@ -501,30 +521,66 @@ class Server:
         return jid
 
     def _admit(self, now: float):
-        while self.queue and len(self.active) < self.max_active and self.queue[0]["arrival"] <= now:
+        while (self.queue and len(self.active) + len(self.building) < self.max_active
+               and self.queue[0]["arrival"] <= now):
             job = self.queue[0]
             need = job_device_bytes(job["cfg"])
-            if self.committed + need > self.budget or need > device_memory()[0]:
+            # the device check also covers builds still allocating
+            if self.committed + need > self.budget or need > device_memory()[0] - self._building_bytes():
                 break
             self.queue.pop(0)
-            job["sim"] = from_config(job["cfg"], output_dir=None)
             job["bytes"] = need
             self.committed += need
             job["admitted"] = now
-            self.active.append(job)
+            shape = _shape_key(job["cfg"])
+            if self._pool is None or shape not in self._shapes:
+                # the first job of a grid shape is built between launches: its
+                # LS solver measures pass plans (LsSolver::tune, cached per
+                # shape), which needs the GPU to itself
+                job["sim"] = from_config(job["cfg"], output_dir=None)
+                self._shapes.add(shape)
+                self.active.append(job)
+            else:
+                job["build"] = self._pool.submit(from_config, job["cfg"], output_dir=None)
+                self.building.append(job)
+                self.built_on_pool += 1
+
+    def _building_bytes(self) -> int:
+        return sum(j["bytes"] for j in self.building)
+
+    def _join_built(self):
+        """Moves finished builds to the active set (in admission order); when
+        nothing is active, waits for the first build instead of idling."""
+        if not self.building:
+            return
+        if not self.active:
+            t0 = time.perf_counter()
+            self.building[0]["build"].result()
+            self.host_seconds["build_wait"] += time.perf_counter() - t0
+        keep = []
+        for job in self.building:
+            if job["build"].done():
+                job["sim"] = job.pop("build").result()  # a failed build raises here
+                self.active.append(job)
+            else:
+                keep.append(job)
+        self.building = keep
 
     def step(self, now: float = 0.0) -> float:
         """One slice; returns the launch's device milliseconds (0 if idle)."""
         self._admit(now)
+        self._join_built()
         if not self.active:
             return 0.0
         ids = [j["id"] for j in self.active]
         if ids != self._batch_ids:  # the active set changed: a new batch (CTA plan) over the resident jobs
+            t0 = time.perf_counter()
             if self._batch is not None:
                 self._batch.close()
             self._batch = KmcBatch(sims=[j["sim"] for j in self.active])
             self._batch.cfgs = [j["cfg"] for j in self.active]
             self._batch_ids = ids
+            self.host_seconds["rebuild"] += time.perf_counter() - t0
         b = self._batch
         # a slice is a device-time budget (every job stops at its first
         # decision past it, so a large job never holds the small ones back),
@@ -535,8 +591,11 @@ class Server:
         else:
             b.set_time_limit(60.0)
             budgets = [min(self.slice_events, j["target"] - j["events"]) for j in self.active]
+        t0 = time.perf_counter()
         ms = b.run(max(budgets), budgets=budgets)
+        self.host_seconds["readback"] += max(0.0, time.perf_counter() - t0 - ms / 1e3)
         self.launches += 1
+        t0 = time.perf_counter()
         keep = []
         for r, job in enumerate(self.active):
             st = b.stats(r)
@@ -564,10 +623,29 @@ class Server:
             b.close()
             self._batch, self._batch_ids = None, None
         self.active = keep
+        self.host_seconds["retire"] += time.perf_counter() - t0
         return ms
 
     def idle(self) -> bool:
-        return not self.queue and not self.active
+        return not self.queue and not self.active and not self.building
+
+    def close(self):
+        """Waits for builds in flight and releases the batch and the pool (the
+        simulations of unfinished jobs are closed)."""
+        if self._pool is not None:
+            self._pool.shutdown(wait=True)
+            self._pool = None
+        for job in self.building:
+            job["sim"] = job.pop("build").result()
+            self.active.append(job)
+        self.building = []
+        if self._batch is not None:
+            self._batch.close()
+            self._batch, self._batch_ids = None, None
+        for job in self.active:
+            if "sim" in job:
+                job["sim"].close()
+                del job["sim"]
 
 
 def kmc_params_from_config(cfg) -> "_lib.KmcParamsC":
@@ -688,14 +766,19 @@ class KmcBatch:
                 "min_margin", "terminated", "ctas", "ms_sweep", "ms_decide", "ms_event_solve", "ms_cascade_flips",
                 "ms_cascade_solve", "ms_interval_end", "sweeps", "h2d_bytes", "d2h_bytes"]
         d = {k: float(v) for k, v in zip(keys, out)}
-        sel = np.zeros(max(ln.value, 1), dtype=np.int32)
-        _lib.check(L.mgk_batch_stats(self._h, r, _lib.dptr(out), sel.ctypes.data_as(_lib.C.POINTER(_lib.C.c_int)),
-                                     sel.size, _lib.C.byref(ln)))
-        d["selected"] = sel[:ln.value].astype(np.int64)
-        _lib.check(L.mgk_batch_event_times(self._h, r, None, 0, _lib.C.byref(ln)))
-        us = np.zeros(max(ln.value, 1))
-        _lib.check(L.mgk_batch_event_times(self._h, r, _lib.dptr(us), us.size, _lib.C.byref(ln)))
-        d["event_us"] = us[:ln.value].copy()
+        n = ln.value
+        if n:
+            sel = np.empty(n, dtype=np.int32)
+            _lib.check(L.mgk_batch_stats(self._h, r, _lib.dptr(out), sel.ctypes.data_as(_lib.C.POINTER(_lib.C.c_int)),
+                                         n, _lib.C.byref(ln)))
+            d["selected"] = sel.astype(np.int64)
+        else:
+            d["selected"] = np.zeros(0, dtype=np.int64)
+        # one event time per logged thermal event (the same count as the log)
+        cap = min(int(d["events"]), 1 << 16)
+        us = np.empty(cap)
+        _lib.check(L.mgk_batch_event_times(self._h, r, _lib.dptr(us) if cap else None, cap, _lib.C.byref(ln)))
+        d["event_us"] = us[:min(ln.value, cap)]
         return d
 
     def field(self, r: int, name: str) -> np.ndarray:

@@ -58,6 +58,14 @@ struct BatchCtl {
     unsigned long long ph_ns[6];              // sweep, decide, event solve, cascade flips, cascade solve, interval end
 };
 
+// What a run call uploads and reads back for one replica, contiguous over the
+// batch so that each direction is one copy for all replicas.
+struct alignas(16) RepState {
+    BatchCtl ctl;
+    rng::Mt mt;
+    unsigned bar[4];  // group barrier {arrivals, generation, error, spare}
+};
+
 struct BatchRep {
     KmcDevState s;
     KmcPhys p;
@@ -173,11 +181,18 @@ template <int D, int C>
 MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
     __shared__ dd sd[32];
     __shared__ int si[32], sl[32];
-    const long NM = R.s.NM;
-    const long m0 = NM * rank / R.ncta, m1 = NM * (rank + 1) / R.ncta;
+    // the replica's state, physics and sweep scratch as locals: the loop
+    // stores Q through a pointer the compiler cannot tell apart from the
+    // BatchRep (global memory), so fields read through R would be reloaded
+    // after every store
+    const KmcDevState st = R.s;
+    const KmcPhys ph = R.p;
+    const int ncta = R.ncta;
+    const long NM = st.NM;
+    const long m0 = NM * rank / ncta, m1 = NM * (rank + 1) / ncta;
     const long ntile = (m1 - m0 + 31) >> 5;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    dd* ts = R.tile_sum + (long)rank * R.tile_cap;
+    dd* const ts = R.tile_sum + (long)rank * R.tile_cap;
     dd acc = {0.0, 0.0};
     int unst = 0, last = -1;
     // four tiles per warp and pass: independent exp / reduction chains in
@@ -191,13 +206,13 @@ MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
             const long i = m0 + (t << 5) + lane;
             r[k] = dd{0.0, 0.0};
             if (t < ntile && i < m1) {
-                const int v = voxel_of(i, NM, R.s.M);
-                const double q = mode_Q<D, C>(R.s, R.p, v, i, time);
-                R.s.Q[i] = q;
+                const int v = voxel_of(i, NM, st.M);
+                const double q = mode_Q<D, C>(st, ph, v, i, time);
+                st.Q[i] = q;
                 bool inc;
-                r[k].hi = rate_of(R.p, q, &inc);
+                r[k].hi = rate_of(ph, q, &inc);
                 if (inc) last = max(last, (int)i);
-                if (q < R.p.threshold) ++unst;
+                if (q < ph.threshold) ++unst;
             }
         }
         // a tile's 32 rates summed in FP64 by a fixed shuffle tree (within a
@@ -867,21 +882,27 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
             }
         } else if (act == ACT_CASCADE) {
             // collect the lowest-Q unstable mode of every unstable voxel
+            // (fields as locals: the stores below would otherwise reload them)
             const long v0 = (long)R.s.N * rank / R.ncta, v1 = (long)R.s.N * (rank + 1) / R.ncta;
+            const double* const Qv = R.s.Q;
+            const int Mv = R.s.M;
+            const double thr = R.p.threshold;
+            double* const ckeys = R.ckeys;
+            int* const cmodes = R.cmodes;
             for (long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
                 double best = 0.0;
                 int bm = -1;
-                for (int m = 0; m < R.s.M; ++m) {
-                    const double q = R.s.Q[v * R.s.M + m];
-                    if (q < R.p.threshold && (bm < 0 || q < best)) {
+                for (int m = 0; m < Mv; ++m) {
+                    const double q = Qv[v * Mv + m];
+                    if (q < thr && (bm < 0 || q < best)) {
                         best = q;
                         bm = m;
                     }
                 }
                 if (bm >= 0) {
                     const int slot = atomicAdd(&c->ccount, 1);
-                    R.ckeys[slot] = best;
-                    R.cmodes[slot] = (int)(v * R.s.M + bm);
+                    ckeys[slot] = best;
+                    cmodes[slot] = (int)(v * Mv + bm);
                 }
             }
             if (!grid_sync(gb)) break;
@@ -1154,15 +1175,63 @@ void BatchEngine::init() {
     int fit = 0;
     BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, batch_kernel, 256, smem_launch));
     if (fit < per_sm) throw std::runtime_error("batch kernel does not fit its planned CTAs per SM");
-    // per-replica device scratch
+    // device scratch of every replica in one allocation (a serving loop
+    // re-plans its batch whenever jobs come and go: one cudaMalloc and one
+    // cudaFree per batch instead of a dozen per replica), carved in two
+    // passes: sizes first, then pointers into the arena
     std::vector<BatchRep> reps(n);
     std::vector<int2> map;
+    for (int r = 0; r < n; ++r)
+        for (int k = 0; k < ncta_[r]; ++k) map.push_back(make_int2(r, k));
+    char* base = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+        size_t off = 0;
+        auto take = [&](size_t bytes) -> void* {
+            void* q = base ? base + off : nullptr;
+            off += (bytes + 255) & ~(size_t)255;
+            return q;
+        };
+        d_state_ = (RepState*)take(sizeof(RepState) * n);
+        d_past_ = (unsigned*)take(2 * sizeof(unsigned));
+        alloc_reps_ = (BatchRep*)take(sizeof(BatchRep) * n);
+        map_ = (int2*)take(sizeof(int2) * map.size());
+        for (int r = 0; r < n; ++r) {
+            KmcEngine& e = *eng_[r];
+            BatchRep& R = reps[r];
+            R.ncta = ncta_[r];
+            R.ctl = &d_state_[r].ctl;
+            R.mt = &d_state_[r].mt;
+            R.bar = d_state_[r].bar;
+            R.past = d_past_;
+            R.chunk_sum = (dd*)take(sizeof(dd) * R.ncta);
+            R.chunk_unst = (int*)take(sizeof(int) * R.ncta);
+            R.chunk_last = (int*)take(sizeof(int) * R.ncta);
+            R.tile_cap = (int)((e.NM_ / R.ncta + 2 + 31) / 32);
+            R.tile_sum = (dd*)take(sizeof(dd) * R.tile_cap * R.ncta);
+            int npow2 = 1;
+            while (npow2 < e.N_) npow2 <<= 1;
+            R.ckeys = (double*)take(sizeof(double) * npow2);
+            R.cmodes = (int*)take(sizeof(int) * npow2);
+            R.ccap = npow2;
+            R.sel_log = (int*)take(sizeof(int) * kSelLog);
+            R.ev_ns = (unsigned long long*)take(sizeof(unsigned long long) * kSelLog);
+            R.ls = plans[r];
+            R.ls.partials = (double*)take(sizeof(double) * kMaxPartials * (R.ncta + 1));
+            R.ls.red = R.ls.partials + (size_t)kMaxPartials * R.ncta;
+            R.ls.result = (LsResult*)take(sizeof(LsResult));
+            R.ls.bar = R.bar;
+            R.ls.err = R.bar + 2;
+        }
+        if (pass == 0) {
+            BCK(cudaMalloc((void**)&arena_, off));
+            base = arena_;
+        }
+    }
     for (int r = 0; r < n; ++r) {
         KmcEngine& e = *eng_[r];
         BatchRep& R = reps[r];
         R.s = e.dev_;
         R.p = e.phys_;
-        R.ls = plans[r];
         R.bg = rng::Barrier{e.bar_.type, e.bar_.mean, e.bar_.std_val, e.bar_.min_cutoff, e.bar_.max_cutoff, e.bar_.loc,
                             e.bar_.scale, e.bar_.epsilon, e.bar_.ratio};
         R.gamma0 = e.p_.gamma0;
@@ -1173,51 +1242,20 @@ void BatchEngine::init() {
         R.rd_dir = e.rd_dir_;
         R.rd_bar = e.rd_bar_;
         R.C = e.C_;
-        R.ncta = ncta_[r];
-        auto alloc = [&](void** p, size_t b) {
-            BCK(cudaMalloc(p, b));
-            owned_.push_back(*p);
-        };
-        alloc((void**)&R.bar, 4 * sizeof(unsigned));
-        alloc((void**)&R.chunk_sum, sizeof(dd) * R.ncta);
-        alloc((void**)&R.chunk_unst, sizeof(int) * R.ncta);
-        alloc((void**)&R.chunk_last, sizeof(int) * R.ncta);
-        R.tile_cap = (int)((e.NM_ / R.ncta + 2 + 31) / 32);
-        alloc((void**)&R.tile_sum, sizeof(dd) * R.tile_cap * R.ncta);
-        int npow2 = 1;
-        while (npow2 < e.N_) npow2 <<= 1;
-        alloc((void**)&R.ckeys, sizeof(double) * npow2);
-        alloc((void**)&R.cmodes, sizeof(int) * npow2);
-        R.ccap = npow2;
-        alloc((void**)&R.mt, sizeof(rng::Mt));
-        alloc((void**)&R.ctl, sizeof(BatchCtl));
-        alloc((void**)&R.sel_log, sizeof(int) * kSelLog);
-        alloc((void**)&R.ev_ns, sizeof(unsigned long long) * kSelLog);
-        alloc((void**)&R.ls.partials, sizeof(double) * kMaxPartials * (R.ncta + 1));
-        R.ls.red = R.ls.partials + (size_t)kMaxPartials * R.ncta;
-        alloc((void**)&R.ls.result, sizeof(LsResult));
-        R.ls.bar = R.bar;
-        R.ls.err = R.bar + 2;
-        BCK(cudaMemset(R.bar, 0, 4 * sizeof(unsigned)));
-        for (int k = 0; k < R.ncta; ++k) map.push_back(make_int2(r, k));
     }
-    BCK(cudaMalloc((void**)&d_past_, 2 * sizeof(unsigned)));
-    for (auto& R : reps) R.past = d_past_;
-    alloc_reps_ = nullptr;
-    BCK(cudaMalloc((void**)&alloc_reps_, sizeof(BatchRep) * n));
+    BCK(cudaMemset(d_state_, 0, sizeof(RepState) * n));
     BCK(cudaMemcpy(alloc_reps_, reps.data(), sizeof(BatchRep) * n, cudaMemcpyHostToDevice));
-    BCK(cudaMalloc((void**)&map_, sizeof(int2) * map.size()));
     BCK(cudaMemcpy(map_, map.data(), sizeof(int2) * map.size(), cudaMemcpyHostToDevice));
+    BCK(cudaMallocHost((void**)&h_state_, sizeof(RepState) * n));
     reps_host_ = reps;
     h2d_.assign(n, 0);
 }
 
 BatchEngine::~BatchEngine() {
     if (st_) cudaStreamSynchronize(st_);
-    for (void* p : owned_) cudaFree(p);
-    cudaFree(alloc_reps_);
-    cudaFree(map_);
-    cudaFree(d_past_);
+    cudaFree(arena_);
+    if (h_state_) cudaFreeHost(h_state_);
+    if (h_logs_) cudaFreeHost(h_logs_);
     eng_.clear();
     owned_eng_.clear();
     if (st_) cudaStreamDestroy(st_);
@@ -1237,13 +1275,7 @@ static void mt_from_host(const std::mt19937& g, rng::Mt* out) {
     out->pad = 0;
 }
 
-static void mt_to_host(const rng::Mt& m, std::mt19937* g) {
-    std::ostringstream os;
-    for (int i = 0; i < 624; ++i) os << m.mt[i] << " ";
-    os << m.idx;
-    std::istringstream is(os.str());
-    is >> *g;
-}
+static_assert(sizeof(rng::Mt) == 626 * sizeof(unsigned), "generator state layout");
 
 mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, double* elapsed_ms) {
     const int n = (int)eng_.size();
@@ -1252,7 +1284,9 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             KmcEngine& e = *eng_[r];
             const mgk_run_params& p = rp[r];
             const int D = e.D_;
-            BatchCtl c{};
+            RepState& hs = h_state_[r];
+            std::memset(&hs, 0, sizeof(RepState));
+            BatchCtl& c = hs.ctl;
             c.time = e.time_;
             std::memcpy(c.eps_macro, e.eps_macro_, sizeof(c.eps_macro));
             std::memcpy(c.sig_macro, e.sig_macro_, sizeof(c.sig_macro));
@@ -1288,14 +1322,11 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             c.sel_log_cap = kSelLog;
             c.t_start_ns = 0;
             c.limit_ns = (unsigned long long)(time_limit_s_ * 1e9);
-            BCK(cudaMemcpyAsync(reps_host_[r].ctl, &c, sizeof(BatchCtl), cudaMemcpyHostToDevice, st_));
-            h2d_[r] = sizeof(BatchCtl) + sizeof(rng::Mt);
-            rng::Mt mt;
-            mt_from_host(e.rng_, &mt);
-            BCK(cudaMemcpyAsync(reps_host_[r].mt, &mt, sizeof(rng::Mt), cudaMemcpyHostToDevice, st_));
-            BCK(cudaMemsetAsync(reps_host_[r].bar, 0, 4 * sizeof(unsigned), st_));
-            BCK(cudaStreamSynchronize(st_));
+            if (e.batch_mt_.size() == 626) std::memcpy(&hs.mt, e.batch_mt_.data(), sizeof(rng::Mt));
+            else mt_from_host(e.rng_, &hs.mt);
+            h2d_[r] = sizeof(RepState);
         }
+        BCK(cudaMemcpyAsync(d_state_, h_state_, sizeof(RepState) * n, cudaMemcpyHostToDevice, st_));
         const unsigned past0[2] = {0u, (unsigned)n};
         BCK(cudaMemcpyAsync(d_past_, past0, sizeof(past0), cudaMemcpyHostToDevice, st_));
         cudaEvent_t e0, e1;
@@ -1306,6 +1337,7 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
         const size_t smem_launch = smem_ + sizeof(rng::Mt) + sizeof(rng::MtRing);
         BCK(cudaLaunchCooperativeKernel((const void*)batch_kernel, dim3(total_ctas_), dim3(256), args, smem_launch, st_));
         cudaEventRecord(e1, st_);
+        BCK(cudaMemcpyAsync(h_state_, d_state_, sizeof(RepState) * n, cudaMemcpyDeviceToHost, st_));
         BCK(cudaStreamSynchronize(st_));
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
@@ -1314,16 +1346,38 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
         if (elapsed_ms) *elapsed_ms = ms;
         mgk_status st = MGK_OK;
         last_.assign(n, BatchStats{});
+        // every replica's event-time and selection logs in one pinned
+        // staging buffer, copied asynchronously, one synchronisation
+        std::vector<size_t> log_off(n + 1, 0);
+        for (int r = 0; r < n; ++r) {
+            const BatchCtl& c = h_state_[r].ctl;
+            const long long ne = std::min<long long>(c.events_done, kSelLog);
+            log_off[r + 1] = log_off[r] + sizeof(unsigned long long) * ne + ((sizeof(int) * c.sel_log_len + 7) & ~(size_t)7);
+        }
+        if (log_off[n] > h_logs_cap_) {
+            if (h_logs_) cudaFreeHost(h_logs_);
+            h_logs_ = nullptr;
+            h_logs_cap_ = 0;
+            BCK(cudaMallocHost((void**)&h_logs_, 2 * log_off[n]));
+            h_logs_cap_ = 2 * log_off[n];
+        }
+        for (int r = 0; r < n; ++r) {
+            const BatchCtl& c = h_state_[r].ctl;
+            const long long ne = std::min<long long>(c.events_done, kSelLog);
+            char* dst = h_logs_ + log_off[r];
+            if (ne)
+                BCK(cudaMemcpyAsync(dst, reps_host_[r].ev_ns, sizeof(unsigned long long) * ne, cudaMemcpyDeviceToHost, st_));
+            if (c.sel_log_len)
+                BCK(cudaMemcpyAsync(dst + sizeof(unsigned long long) * ne, reps_host_[r].sel_log, sizeof(int) * c.sel_log_len,
+                                    cudaMemcpyDeviceToHost, st_));
+        }
+        BCK(cudaStreamSynchronize(st_));
         for (int r = 0; r < n; ++r) {
             KmcEngine& e = *eng_[r];
-            BatchCtl c;
-            unsigned bar[4];
-            rng::Mt mt;
-            BCK(cudaMemcpy(&c, reps_host_[r].ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost));
-            BCK(cudaMemcpy(bar, reps_host_[r].bar, sizeof(bar), cudaMemcpyDeviceToHost));
-            BCK(cudaMemcpy(&mt, reps_host_[r].mt, sizeof(rng::Mt), cudaMemcpyDeviceToHost));
-            long long d2h = sizeof(BatchCtl) + sizeof(bar) + sizeof(rng::Mt);
-            if (bar[2]) {
+            const BatchCtl& c = h_state_[r].ctl;
+            const rng::Mt& mt = h_state_[r].mt;
+            long long d2h = sizeof(RepState);
+            if (h_state_[r].bar[2]) {
                 last_error = "device wait timed out in the batched kernel";
                 st = MGK_DEVICE_TIMEOUT;
             }
@@ -1332,7 +1386,8 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             std::memcpy(e.eps_macro_, c.eps_macro, sizeof(c.eps_macro));
             std::memcpy(e.sig_macro_, c.sig_macro, sizeof(c.sig_macro));
             for (int k = 0; k < 3; ++k) e.ls_->w_[k] = c.w[k], e.ls_->asym_dev2_[k] = 0.0;
-            mt_to_host(mt, &e.rng_);
+            e.batch_mt_.resize(626);
+            std::memcpy(e.batch_mt_.data(), &mt, sizeof(rng::Mt));
             e.batch_started = true;
             e.batch_remaining = c.remaining;
             BatchStats& b = last_[r];
@@ -1354,15 +1409,13 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             for (int k = 0; k < 6; ++k) b.phase_ms[k] = 1e-6 * (double)c.ph_ns[k];
             {
                 const long long ne = std::min<long long>(c.events_done, kSelLog);
-                std::vector<unsigned long long> t(ne);
-                if (ne) BCK(cudaMemcpy(t.data(), reps_host_[r].ev_ns, sizeof(unsigned long long) * ne, cudaMemcpyDeviceToHost));
+                const unsigned long long* t = reinterpret_cast<const unsigned long long*>(h_logs_ + log_off[r]);
                 d2h += (long long)sizeof(unsigned long long) * ne;
                 b.event_us.resize(ne);
                 for (long long i = 0; i < ne; ++i) b.event_us[i] = 1e-3 * (double)(t[i] - (i ? t[i - 1] : c.t_start_ns));
+                const int* sel = reinterpret_cast<const int*>(h_logs_ + log_off[r] + sizeof(unsigned long long) * ne);
+                b.sel.assign(sel, sel + c.sel_log_len);
             }
-            b.sel.resize(c.sel_log_len);
-            if (c.sel_log_len)
-                BCK(cudaMemcpy(b.sel.data(), reps_host_[r].sel_log, sizeof(int) * c.sel_log_len, cudaMemcpyDeviceToHost));
             d2h += (long long)sizeof(int) * c.sel_log_len;
             b.h2d_bytes = h2d_[r];
             b.d2h_bytes = d2h;

@@ -10,6 +10,7 @@
 namespace mgk {
 
 struct BatchRep;
+struct RepState;
 constexpr int kSelLog = 1 << 16;  // selected-mode log entries kept per replica and run
 
 struct BatchStats {
@@ -56,13 +57,17 @@ private:
     std::vector<KmcEngine*> eng_;
     std::vector<std::unique_ptr<KmcEngine>> owned_eng_;
     std::vector<int> ncta_;
-    std::vector<void*> owned_;
+    char* arena_ = nullptr;       // every replica's device scratch (one allocation)
+    RepState* d_state_ = nullptr;  // per replica: control block, generator, barrier words (in the arena)
+    RepState* h_state_ = nullptr;  // pinned host copy of d_state_
+    char* h_logs_ = nullptr;       // pinned staging of the run's event-time and selection logs
+    size_t h_logs_cap_ = 0;
     std::vector<BatchRep> reps_host_;
     std::vector<long long> h2d_;
     std::vector<BatchStats> last_;
     BatchRep* alloc_reps_ = nullptr;
     int2* map_ = nullptr;
-    unsigned* d_past_ = nullptr;  // {replicas past the time limit or finished, replicas}
+    unsigned* d_past_ = nullptr;  // {replicas past the time limit or finished, replicas} (in the arena)
     size_t smem_ = 0;
     int total_ctas_ = 0;
     double time_limit_s_ = 60.0;

@@ -9,6 +9,7 @@
 // enqueues select+flip, the warm-started LS solve and the next sweep in one go.
 #include <chrono>
 #include <cmath>
+#include <sstream>
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
@@ -717,7 +718,19 @@ void KmcEngine::maybe_vtk(int global_step, int elastic_steps_done, const char* t
     export_vtu(name);
 }
 
+void KmcEngine::sync_host_rng() {
+    if (batch_mt_.empty()) return;
+    // std::mt19937's text form: the 624 state words, then the index
+    std::ostringstream os;
+    for (int i = 0; i < 624; ++i) os << batch_mt_[i] << " ";
+    os << batch_mt_[624];
+    std::istringstream is(os.str());
+    is >> rng_;
+    batch_mt_.clear();
+}
+
 mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap, long long* rows_out) {
+    sync_host_rng();
     const int D = D_, DD = D * D;
     long long rows = 0;
     auto push = [&](double kind, double a, double b, double R, double tw) {

@@ -93,6 +93,12 @@ private:
     KmcPhys phys_{};
     BarrierGen bar_;
     std::mt19937 rng_;
+    // While batched runs own the generator, its state stays in their layout
+    // (624 state words, the index, a pad word) and rng_ is brought up to date
+    // from it only when the plain form draws again: a serving loop runs many
+    // short batched runs back to back.  Empty: rng_ is current.
+    std::vector<unsigned> batch_mt_;
+    void sync_host_rng();
     std::vector<double> E_, nu_;
     double eps_macro_[9] = {0}, sig_macro_[9] = {0};
     double time_ = 0.0;

@@ -152,3 +152,39 @@ def test_batch_time_limit_mixed_sizes(G, tmp_path):
     assert st_s["terminated"] == 2 and st_b["terminated"] == 2
     assert st_s["events"] > 0 and st_s["event_us"].sum() / 1e3 > 0.8 * 200.0
     assert np.isfinite(b.field(0, "eps_field")).all() and np.isfinite(b.field(1, "eps_field")).all()
+
+
+def test_generator_handed_between_batched_and_plain_runs(G, tmp_path):
+    """Between batched runs the generator stays in the device layout and is
+    handed back to the plain form only when that form draws again: split
+    batched runs select what one run selects, and a plain run after them
+    continues the same stream as a plain run after plain runs of the same
+    events."""
+    from mgkmc_cpp_b200 import workloads
+    cfg = workloads.write_workload("ens2d_64", str(tmp_path), seed=3)[1]
+    kw = dict(enable_console_log=False, enable_summary_log=False, enable_global_log=False)
+
+    def plain(sim, nev):
+        tr = sim.run_simulation(10 ** 6, cfg.step_size, cfg.driving, cfg.targets, cfg.mixed_tol_pa, 50,
+                                max_events=nev, trace=True, **kw)
+        return events_of(tr)
+
+    a = G.from_config(cfg, output_dir=None)
+    ba = G.KmcBatch(sims=[a])
+    ba.run(40)
+    sel_a = ba.stats(0)["selected"]
+    ba.close()
+    b = G.from_config(cfg, output_dir=None)
+    parts = []
+    for nev in (15, 25):  # two batches over the same simulation, one run each
+        bb = G.KmcBatch(sims=[b])
+        bb.run(nev)
+        parts.append(bb.stats(0)["selected"])
+        bb.close()
+    assert np.array_equal(np.concatenate(parts), sel_a)
+    e = G.from_config(cfg, output_dir=None)
+    assert np.array_equal(plain(e, 40), sel_a)
+    after_e = plain(e, 10)
+    assert len(after_e) == 10
+    assert np.array_equal(plain(a, 10), after_e)
+    assert np.array_equal(plain(b, 10), after_e)

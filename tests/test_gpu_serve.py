@@ -97,3 +97,28 @@ def test_admission_gated_by_free_memory(G, tmp_path):
         assert srv.committed <= srv.budget
     assert len(srv.done) == 3
     assert srv.launches == 3
+
+
+def test_jobs_built_on_the_pool_same_as_alone(G, tmp_path):
+    """build_threads > 0: jobs after the first of their grid shape are built
+    on host threads while the others run, and join the batch when ready; each
+    still selects exactly its own modes."""
+    seeds = [3, 4, 5, 6, 7, 8]
+    cfgs = [_cfg("ens2d_64" if s % 2 else "ens2d_128", s, tmp_path) for s in seeds]
+    targets = [60, 40, 50, 30, 45, 35]
+    refs = []
+    for c, t in zip(cfgs, targets):
+        b = G.KmcBatch([c])
+        b.run(t)
+        refs.append(b.stats(0)["selected"])
+        b.close()
+    srv = G.Server(slice_seconds=0.002, build_threads=2)
+    ids = [srv.submit(c, t) for c, t in zip(cfgs, targets)]
+    while not srv.idle():
+        srv.step()
+    srv.close()
+    assert srv.built_on_pool == 4  # every job after the first of its grid shape
+    for jid, ref in zip(ids, refs):
+        assert np.array_equal(srv.done[jid]["selected"], ref)
+    assert srv.committed == 0
+    assert set(srv.host_seconds) == {"build_wait", "rebuild", "readback", "retire"}
