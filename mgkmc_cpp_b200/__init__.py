@@ -746,10 +746,15 @@ class KmcBatch:
         the kernel time in milliseconds.  A run that reaches the time limit
         returns normally with ``self.time_limited`` set."""
         n = len(self.cfgs)
-        rps = (_lib.RunParamsC * n)(*[run_params_from_config(c, n_global_steps, max_cascade_batches) for c in self.cfgs])
-        if budgets is not None:
-            for r, b in enumerate(budgets):
-                rps[r].max_events = int(b)
+        key = (int(n_global_steps), int(max_cascade_batches), tuple(id(c) for c in self.cfgs))
+        cache = getattr(self, "_rps", None)
+        if cache is None or cache[0] != key:  # the run parameters, built once per batch and kind of call
+            rps = (_lib.RunParamsC * n)(*[run_params_from_config(c, n_global_steps, max_cascade_batches)
+                                          for c in self.cfgs])
+            self._rps = (key, rps)
+        rps = self._rps[1]
+        for r in range(n):
+            rps[r].max_events = int(budgets[r]) if budgets is not None else 0
         ms = np.zeros(1)
         st = _lib.lib().mgk_batch_run(self._h, rps, int(max_events), _lib.dptr(ms))
         self.time_limited = st == 9

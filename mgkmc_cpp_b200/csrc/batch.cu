@@ -1295,11 +1295,8 @@ mgk_status BatchEngine::run(const mgk_run_params* rp, long long max_events, doub
             c.dt_step = std::fabs(p.step_size) / e.p_.strain_rate;
             c.strain_rate = e.p_.strain_rate;
             c.sum_two_mu = e.ls_->sum_two_mu_;
-            double Es = 0.0, ns = 0.0;
-            for (double v : e.E_) Es += v;
-            for (double v : e.nu_) ns += v;
-            c.Ea = Es / e.E_.size();
-            c.na = ns / e.nu_.size();
+            c.Ea = e.E_avg_;
+            c.na = e.nu_avg_;
             c.mixed_tol = p.mixed_tol;
             c.mixed_max_iter = p.mixed_max_iter;
             c.ls_tol = e.p_.ls_tol;

@@ -99,6 +99,13 @@ KmcEngine::KmcEngine(const mgk_kmc_params& p, const double* E, const double* nu)
     NM_ = N * M_;
     E_.assign(E, E + N);
     nu_.assign(nu, nu + N);
+    {
+        double Es = 0.0, ns = 0.0;
+        for (double v : E_) Es += v;
+        for (double v : nu_) ns += v;
+        E_avg_ = Es / E_.size();
+        nu_avg_ = ns / nu_.size();
+    }
     CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     int dims[3] = {p.nx, p.ny, D_ == 3 ? p.nz : 1};
     ls_.reset(new LsSolver(D_, dims, p.plane_stress != 0, p.pixel, E, nu, st_));
@@ -653,9 +660,7 @@ void KmcEngine::log_line(int global_step, int elastic_steps_done, int total_kmc,
         if (D == 2) {
             double sig_zz = 0.0;
             if (!p_.plane_stress) {
-                double ns = 0.0;
-                for (double v : nu_) ns += v;
-                sig_zz = (ns / nu_.size()) * (sig_macro_[0] + sig_macro_[3]);
+                sig_zz = nu_avg_ * (sig_macro_[0] + sig_macro_[3]);
             }
             snprintf(g, sizeof(g),
                      "%-10d %-12d %-10d %-15.6f %-15.6f %-15.6f %-15.6f %-15.6f %-15.6f %-15.3f %-15.3f %-15.3f %-15.3f %-15.3f "
@@ -891,10 +896,7 @@ mgk_status KmcEngine::run(const mgk_run_params& rp, double* trace, long long cap
             }
             if (stop) break;
             // mixed boundary conditions (kmc_solver.hpp:955-987)
-            double Es = 0.0, ns = 0.0;
-            for (double v : E_) Es += v;
-            for (double v : nu_) ns += v;
-            const double Ea = Es / E_.size(), na = ns / nu_.size();
+            const double Ea = E_avg_, na = nu_avg_;
             int solves = 0;
             for (int it = 0; it < rp.mixed_max_iter; ++it) {
                 s = elastic_run();

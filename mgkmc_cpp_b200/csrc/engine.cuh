@@ -100,6 +100,7 @@ private:
     std::vector<unsigned> batch_mt_;
     void sync_host_rng();
     std::vector<double> E_, nu_;
+    double E_avg_ = 0.0, nu_avg_ = 0.0;  // means of E_ and nu_ (left-to-right sums), for the mixed-BC update
     double eps_macro_[9] = {0}, sig_macro_[9] = {0};
     double time_ = 0.0;
     // device scratch
