@@ -75,6 +75,7 @@ struct BatchRep {
     int redraw_dir, redraw_bar, C, pad0;
     int ext, rd_dir, rd_bar, pad1;  // catalog / per-voxel barrier extensions and their RD_* redraw modes
     int ls_prec, pad2;              // LS re-solves: 0 FP64, 1 FP32-refined
+    unsigned long long wait_ns;     // limit of one wait at the group's barriers
     int ncta;
     unsigned* bar;  // {arrivals, generation, error, spare}
     dd* chunk_sum;
@@ -176,61 +177,87 @@ __device__ __noinline__ bool group_solve(BatchRep& R, int rank, const GridBar& g
 // (update_barriers + the rate block, kmc_solver.hpp:341-410, :783-803), with
 // each warp handling 32-mode tiles: the tile's rate sum goes to tile_sum, the
 // chunk's sum (double-double over tiles), unstable count and last included
-// mode to the chunk arrays.
+// mode to the chunk arrays.  The chunk runs in pieces of whole tiles: the
+// CTA first writes the voxel terms of the piece's voxels (stress, softening
+// level, for the directional scheme the previous flip) to shared memory, then
+// the modes read them there, so a mode loads only its barrier and catalog
+// entry.  Warp w takes tiles w, w + nw, ... of the chunk in increasing order
+// in every piece, so the sums are added in the same order whatever the pieces.
 template <int D, int C>
-MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time) {
+MGK_DEV void sweep_chunk(BatchRep& R, int rank, double time, unsigned char* smem, size_t smem_bytes) {
+    constexpr int S = D == 2 ? 3 : 6;
     __shared__ dd sd[32];
     __shared__ int si[32], sl[32];
-    // the replica's state, physics and sweep scratch as locals: the loop
-    // stores Q through a pointer the compiler cannot tell apart from the
-    // BatchRep (global memory), so fields read through R would be reloaded
-    // after every store
+    // the replica's state, physics and sweep scratch as locals (read once)
     const KmcDevState st = R.s;
     const KmcPhys ph = R.p;
     const int ncta = R.ncta;
     const long NM = st.NM;
+    const int M = st.M;
     const long m0 = NM * rank / ncta, m1 = NM * (rank + 1) / ncta;
     const long ntile = (m1 - m0 + 31) >> 5;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     dd* const ts = R.tile_sum + (long)rank * R.tile_cap;
+    // voxel record: sg[S], gb, then (directional) ps[S], npv
+    const int rec = ph.directional ? 2 * S + 2 : S + 1;
+    double* const vx = reinterpret_cast<double*>(smem);
+    const long cap_vox = (long)(smem_bytes / (sizeof(double) * rec));
+    // a run of 32 T modes touches at most 32 T / M + 2 voxels
+    const long T = max(1L, ((cap_vox - 2) * M) / 32);
     dd acc = {0.0, 0.0};
     int unst = 0, last = -1;
     // four tiles per warp and pass: independent exp / reduction chains in
     // flight (two 256-thread CTAs per SM leave only 16 warps to hide latency)
     constexpr int U = 4;
-    for (long tb = wid; tb < ntile; tb += (long)nw * U) {
-        dd r[U];
-#pragma unroll
-        for (int k = 0; k < U; ++k) {
-            const long t = tb + (long)k * nw;
-            const long i = m0 + (t << 5) + lane;
-            r[k] = dd{0.0, 0.0};
-            if (t < ntile && i < m1) {
-                const int v = voxel_of(i, NM, st.M);
-                const double q = mode_Q<D, C>(st, ph, v, i, time);
-                st.Q[i] = q;
-                bool inc;
-                r[k].hi = rate_of(ph, q, &inc);
-                if (inc) last = max(last, (int)i);
-                if (q < ph.threshold) ++unst;
-            }
+    for (long T0 = 0; T0 < ntile; T0 += T) {
+        const long T1 = min(ntile, T0 + T);
+        const long mlo = m0 + (T0 << 5), mhi = min(m1, m0 + (T1 << 5));
+        const int vlo = voxel_of(mlo, NM, M), vhi = voxel_of(mhi - 1, NM, M);
+        for (int v = vlo + (int)threadIdx.x; v <= vhi; v += blockDim.x) {
+            double* r = vx + (long)(v - vlo) * rec;
+            sweep_stress<D>(st, v, r);
+            r[S] = voxel_gb<D, C>(st, ph, v, time);
+            if (ph.directional) r[2 * S + 1] = voxel_prev<D, C>(st, v, r + S + 1);
         }
-        // a tile's 32 rates summed in FP64 by a fixed shuffle tree (within a
-        // few ulp of the tile sum, far tighter than the reference's serial
-        // sum over all modes); tiles accumulate in double-double
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-            for (int k = 0; k < U; ++k) r[k].hi += __shfl_down_sync(0xffffffffu, r[k].hi, o);
-        if (lane == 0)
+        __syncthreads();
+        const long tfirst = T0 + ((long)wid - T0 % nw + nw) % nw;
+        for (long tb = tfirst; tb < T1; tb += (long)nw * U) {
+            dd r[U];
 #pragma unroll
             for (int k = 0; k < U; ++k) {
                 const long t = tb + (long)k * nw;
-                if (t < ntile) {
-                    ts[t] = r[k];
-                    acc = dd_add(acc, r[k]);
+                const long i = m0 + (t << 5) + lane;
+                r[k] = dd{0.0, 0.0};
+                if (t < T1 && i < m1) {
+                    const int v = voxel_of(i, NM, M);
+                    const double* vr = vx + (long)(v - vlo) * rec;
+                    const double q = mode_Q_terms<D, C>(st, ph, v, i, vr, vr[S], vr + S + 1,
+                                                        ph.directional ? vr[2 * S + 1] : 0.0, st.Q0[i]);
+                    st.Q[i] = q;
+                    bool inc;
+                    r[k].hi = rate_of(ph, q, &inc);
+                    if (inc) last = max(last, (int)i);
+                    if (q < ph.threshold) ++unst;
                 }
             }
+            // a tile's 32 rates summed in FP64 by a fixed shuffle tree (within a
+            // few ulp of the tile sum, far tighter than the reference's serial
+            // sum over all modes); tiles accumulate in double-double
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int k = 0; k < U; ++k) r[k].hi += __shfl_down_sync(0xffffffffu, r[k].hi, o);
+            if (lane == 0)
+#pragma unroll
+                for (int k = 0; k < U; ++k) {
+                    const long t = tb + (long)k * nw;
+                    if (t < T1) {
+                        ts[t] = r[k];
+                        acc = dd_add(acc, r[k]);
+                    }
+                }
+        }
+        __syncthreads();  // the next piece overwrites the voxel records
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -831,7 +858,7 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
     rng::MtRing& s_ring = *reinterpret_cast<rng::MtRing*>(smem + smem_bytes + sizeof(rng::Mt));
     __shared__ int s_flag;
     BatchCtl* c = R.ctl;
-    const GridBar gb{R.bar, (unsigned)R.ncta, R.bar + 2, kBarrierTimeoutNs};
+    const GridBar gb{R.bar, (unsigned)R.ncta, R.bar + 2, R.wait_ns};
     if (rank == 0) {
         for (int i = threadIdx.x; i < 624; i += blockDim.x) s_mt.mt[i] = R.mt->mt[i];
         if (threadIdx.x == 0) s_mt.idx = R.mt->idx;
@@ -858,7 +885,7 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
     };
     while (ok) {
         if (vld(&c->done)) break;
-        sweep_chunk<D, C>(R, rank, c->time);
+        sweep_chunk<D, C>(R, rank, c->time, smem, smem_bytes);
         if (!grid_sync(gb)) break;
         if (timer) c->sweeps++;
         phase(0);
@@ -922,8 +949,16 @@ MGK_DEV void run_replica(BatchRep& R, int rank, unsigned char* smem, size_t smem
                 int npow2 = 1;
                 while (npow2 < n) npow2 <<= 1;
                 if ((size_t)npow2 * 12 <= smem_bytes) cta_sort(R.ckeys, R.cmodes, n, smem, smem_bytes);
-                if (threadIdx.x == 0)
-                    for (int f = 0; f < n; ++f) apply_flip<D, C>(R.s, R.p, R.cmodes[f], c->time, nullptr);
+                if (threadIdx.x == 0) {
+                    // state as locals: the flips store through pointers that
+                    // could otherwise alias the replica record and the control
+                    // block, and reload them at every flip
+                    const KmcDevState st = R.s;
+                    const KmcPhys ph = R.p;
+                    const int* const cm = R.cmodes;
+                    const double tnow = c->time;
+                    for (int f = 0; f < n; ++f) apply_flip<D, C>(st, ph, cm[f], tnow, nullptr);
+                }
                 __syncthreads();
                 // flips touch no other voxel's catalog or barriers, so all
                 // redraws may follow all flips (same draws, same order)
@@ -1242,6 +1277,12 @@ void BatchEngine::init() {
         R.rd_dir = e.rd_dir_;
         R.rd_bar = e.rd_bar_;
         R.C = e.C_;
+        // the longest phase the group's other CTAs wait through is rank 0's
+        // part of a cascade batch (flips one after another, then the redraw
+        // of every mode): its limit grows with the grid, so an avalanche
+        // through a large 3D grid (every voxel unstable, 100 modes each) is
+        // not taken for a stalled group
+        R.wait_ns = kBarrierTimeoutNs + 20000ull * (unsigned long long)e.N_ + 4000ull * (unsigned long long)e.NM_;
     }
     BCK(cudaMemset(d_state_, 0, sizeof(RepState) * n));
     BCK(cudaMemcpy(alloc_reps_, reps.data(), sizeof(BatchRep) * n, cudaMemcpyHostToDevice));

@@ -121,14 +121,11 @@ MGK_DEV void sweep_stress(const KmcDevState& s, int v, double* sg) {
     }
 }
 
-// Q of mode i at voxel v (update_barriers, kmc_solver.hpp:345-407 / :1344-1406)
+// The voxel-only terms of update_barriers (kmc_solver.hpp:345-407 /
+// :1344-1406): the softening level of voxel v now (decayed transient part plus
+// the permanent part, capped) ...
 template <int D, int C>
-MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, double time) {
-    constexpr int S = D == 2 ? 3 : 6;
-    const int N = s.N;
-    double sg[S];
-    sweep_stress<D>(s, v, sg);
-    // softening state
+MGK_DEV double voxel_gb(const KmcDevState& s, const KmcPhys& p, int v, double time) {
     const double gt = s.soft[2 * v + 1];
     double gtc = 0.0;
     if (gt > 0.0) {
@@ -143,21 +140,39 @@ MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, dou
     }
     double gb = s.soft[2 * v] + gtc;
     if (p.softening_cap > 0.0 && gb > p.softening_cap) gb = p.softening_cap;
+    return gb;
+}
+
+// ... and, for the directional scheme, the symmetric components of the
+// voxel's previous flip and their norm.
+template <int D, int C>
+MGK_DEV double voxel_prev(const KmcDevState& s, int v, double* ps) {
+    constexpr int S = D == 2 ? 3 : 6;
+    cat_sym<D, C>(s.prev + (long)v * C, ps);
+    double np = 0.0;
+#pragma unroll
+    for (int c = 0; c < S; ++c) np += (c < D ? 1.0 : 2.0) * ps[c] * ps[c];
+    return sqrt(np);
+}
+
+// Q of mode i at voxel v from the voxel terms (stress sg, softening gb, and
+// for the directional scheme ps / npv) and the mode's barrier q0.
+template <int D, int C>
+MGK_DEV double mode_Q_terms(const KmcDevState& s, const KmcPhys& p, int v, long i, const double* sg, double gb,
+                            const double* ps, double npv, double q0) {
+    constexpr int S = D == 2 ? 3 : 6;
     double cs[S];
     mode_eps<D, C>(s, v, i, sg, cs);
     double mod = 1.0;
     if (p.directional) {
-        double ps[S];
-        cat_sym<D, C>(s.prev + (long)v * C, ps);
-        double dp = 0.0, nm = 0.0, np = 0.0;
+        double dp = 0.0, nm = 0.0;
 #pragma unroll
         for (int c = 0; c < S; ++c) {
             const double wgt = c < D ? 1.0 : 2.0;
             dp += wgt * cs[c] * ps[c];
             nm += wgt * cs[c] * cs[c];
-            np += wgt * ps[c] * ps[c];
         }
-        const double npv = sqrt(np), nmv = sqrt(nm);
+        const double nmv = sqrt(nm);
         if (!(npv < 1e-12 || nmv < 1e-12)) {
             const double ct = dp / (nmv * npv);
             mod = (1.0 + ct) * (1.0 + ct) / 4.0;
@@ -169,7 +184,20 @@ MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, dou
     for (int c = 0; c < S; ++c) w += (c < D ? 1.0 : 2.0) * sg[c] * cs[c];
     const double wv = 0.5 * p.volume * (w / 1e9) * 6.241509;
     // exp(-0) is exactly 1: skip the exponential for unsoftened voxels
-    return (geff == 0.0 ? s.Q0[i] : s.Q0[i] * exp(-geff)) - wv;
+    return (geff == 0.0 ? q0 : q0 * exp(-geff)) - wv;
+}
+
+// Q of mode i at voxel v (update_barriers, kmc_solver.hpp:345-407 / :1344-1406)
+template <int D, int C>
+MGK_DEV double mode_Q(const KmcDevState& s, const KmcPhys& p, int v, long i, double time) {
+    constexpr int S = D == 2 ? 3 : 6;
+    double sg[S];
+    sweep_stress<D>(s, v, sg);
+    const double gb = voxel_gb<D, C>(s, p, v, time);
+    double ps[S];
+    double npv = 0.0;
+    if (p.directional) npv = voxel_prev<D, C>(s, v, ps);
+    return mode_Q_terms<D, C>(s, p, v, i, sg, gb, ps, npv, s.Q0[i]);
 }
 
 MGK_DEV double rate_of(const KmcPhys& p, double q, bool* inc) {
