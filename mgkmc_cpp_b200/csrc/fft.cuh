@@ -147,9 +147,12 @@ MGK_DEV void fft_stage(const cplx<T>* __restrict__ in, cplx<T>* __restrict__ out
 
 // Runs all stages of `ax` over `nlines` lines held in `a`; `b` is scratch of the
 // same size.  Returns the buffer that holds the result.  Contains __syncthreads.
+// tw_s: a shared-memory copy of the axis twiddle table (load_twiddles), or
+// null to read the table from global memory.
 template <typename T>
-__device__ __noinline__ cplx<T>* fft_lines(cplx<T>* a, cplx<T>* b, int nlines, const FftAxis& ax, int sign) {
-    const cplx<T>* tw = tw_of<T>(ax);
+__device__ __noinline__ cplx<T>* fft_lines(cplx<T>* a, cplx<T>* b, int nlines, const FftAxis& ax, int sign,
+                                           const cplx<T>* tw_s = nullptr) {
+    const cplx<T>* tw = tw_s ? tw_s : tw_of<T>(ax);
     int Ns = 1;
     for (int s = 0; s < ax.nst; ++s) {
         const int R = ax.radix[s];
@@ -246,11 +249,10 @@ __device__ __noinline__ cplx<T>* fft_lines_warp(cplx<T>* a, cplx<T>* b, int nlin
     return (ax.nst & 1) ? b : a;
 }
 
-// Copies the axis twiddle table to shared memory (warp-owned path); the
-// caller synchronises before use.
+// Copies the axis twiddle table to shared memory (both transform paths read
+// it there); the caller synchronises before use.
 template <typename T>
 MGK_DEV void load_twiddles(const FftAxis& ax, cplx<T>* tw_s) {
-    if (ax.lw == 0) return;
     const cplx<T>* tw = tw_of<T>(ax);
     for (int i = threadIdx.x; i < ax.n; i += blockDim.x) tw_s[i] = tw[i];
 }
@@ -261,7 +263,7 @@ MGK_DEV void load_twiddles(const FftAxis& ax, cplx<T>* tw_s) {
 template <typename T>
 MGK_DEV cplx<T>* fft_any(cplx<T>* a, cplx<T>* b, int nlines, const FftAxis& ax, const cplx<T>* tw_s, int sign) {
     if (ax.lw > 0) return fft_lines_warp<T>(a, b, nlines, pad_len(ax.n), ax, tw_s, sign);
-    return fft_lines<T>(a, b, nlines, ax, sign);
+    return fft_lines<T>(a, b, nlines, ax, sign, tw_s);
 }
 
 }  // namespace mgk
