@@ -44,6 +44,12 @@ MGK_API int mgk_device_count(void);
 /* Free and total memory of the current device, in bytes (admission control of
  * a request loop). */
 MGK_API mgk_status mgk_device_memory(unsigned long long* free_bytes, unsigned long long* total_bytes);
+/* The calling thread's current CUDA device (every handle's device state is
+ * created there), and setting it: a host thread that builds simulations for
+ * another thread's GPU first adopts that thread's device.  No counterpart in
+ * the reference (single-GPU, single-threaded). */
+MGK_API mgk_status mgk_get_device(int* device);
+MGK_API mgk_status mgk_set_device(int device);
 
 /* ---------------------------------------------------------------- LS solver
  * Replaces spectral_solver_2d (linear_elastic_solver.hpp:146-160) and

@@ -466,6 +466,19 @@ def _shape_key(cfg):
     return (cfg.dim, cfg.nx, cfg.ny, cfg.nz if cfg.dim == 3 else 1, cfg.plane_mode)
 
 
+def current_device() -> int:
+    """The calling thread's CUDA device (mgk_get_device)."""
+    d = _lib.C.c_int(0)
+    _lib.check(_lib.lib().mgk_get_device(_lib.C.byref(d)))
+    return d.value
+
+
+def _build_on(device: int, cfg):
+    # a pool thread starts on device 0: adopt the submitting thread's device
+    _lib.check(_lib.lib().mgk_set_device(int(device)))
+    return from_config(cfg, output_dir=None)
+
+
 class Server:
     """Continuous batching of KMC jobs on one GPU (the serving loop).
 
@@ -541,7 +554,7 @@ class Server:
                 self._shapes.add(shape)
                 self.active.append(job)
             else:
-                job["build"] = self._pool.submit(from_config, job["cfg"], output_dir=None)
+                job["build"] = self._pool.submit(_build_on, current_device(), job["cfg"])
                 self.building.append(job)
                 self.built_on_pool += 1
 

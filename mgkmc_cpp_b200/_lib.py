@@ -21,7 +21,7 @@ EXPORTS = ["mgk_last_error", "mgk_version", "mgk_device_count", "mgk_ls_create",
            "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro", "mgk_batch_set_time_limit", "mgk_batch_event_times", "mgk_le_run",
            "mgk_batch_create_from", "mgk_device_memory", "mgk_correlated_field",
            "mgk_ls_set_precision", "mgk_ls_last_solve_ms", "mgk_ls_set_wait_limit", "mgk_ls_inject_absent_cta", "mgk_ls_plan", "mgk_set_batch_plan",
-           "mgk_batch_destroy"]
+           "mgk_get_device", "mgk_set_device", "mgk_batch_destroy"]
 
 
 class MgkError(RuntimeError):
@@ -109,6 +109,8 @@ def lib():
     L.mgk_ls_inject_absent_cta.argtypes = [vp, C.c_int]
     L.mgk_ls_plan.argtypes = [vp, C.POINTER(C.c_int)]
     L.mgk_set_batch_plan.argtypes = [C.c_int]
+    L.mgk_get_device.argtypes = [C.POINTER(C.c_int)]
+    L.mgk_set_device.argtypes = [C.c_int]
     L.mgk_le_run.argtypes = [C.POINTER(LeParamsC), dp, dp, dp, C.POINTER(C.c_int)]
     L.mgk_batch_event_times.argtypes = [vp, C.c_int, dp, C.c_longlong, C.POINTER(C.c_longlong)]
     L.mgk_batch_destroy.argtypes = [vp]
@@ -120,7 +122,8 @@ def lib():
                "mgk_batch_create", "mgk_batch_run", "mgk_batch_stats", "mgk_batch_get_field", "mgk_batch_get_macro",
                "mgk_batch_set_time_limit", "mgk_batch_event_times", "mgk_le_run",
                "mgk_batch_create_from", "mgk_device_memory", "mgk_correlated_field",
-               "mgk_ls_set_precision", "mgk_ls_last_solve_ms", "mgk_ls_set_wait_limit", "mgk_ls_inject_absent_cta", "mgk_ls_plan", "mgk_set_batch_plan"):
+               "mgk_ls_set_precision", "mgk_ls_last_solve_ms", "mgk_ls_set_wait_limit", "mgk_ls_inject_absent_cta", "mgk_ls_plan", "mgk_set_batch_plan",
+               "mgk_get_device", "mgk_set_device"):
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L

@@ -320,6 +320,21 @@ mgk_status mgk_batch_create_from(mgk_batch** out, int n, mgk_kmc* const* sims) {
     return MGK_OK;
 }
 
+mgk_status mgk_get_device(int* device) {
+    if (!device) return fail(MGK_BAD_ARG, "null device pointer");
+    cudaError_t e = cudaGetDevice(device);
+    if (e != cudaSuccess) return fail(MGK_CUDA_ERROR, cudaGetErrorString(e));
+    return MGK_OK;
+}
+
+mgk_status mgk_set_device(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return fail(MGK_BAD_ARG, "no such device");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(MGK_CUDA_ERROR, cudaGetErrorString(e));
+    return MGK_OK;
+}
+
 mgk_status mgk_device_memory(unsigned long long* free_bytes, unsigned long long* total_bytes) {
     size_t f = 0, t = 0;
     cudaError_t e = cudaMemGetInfo(&f, &t);
