@@ -142,3 +142,55 @@ def test_close_releases_jobs_still_building(fakes, tmp_path):
     assert srv.building == [] and srv._pool is None
     assert all(s.closed for s in sims_before if s is not None)
     assert all("sim" not in j for j in srv.active)
+
+
+def test_bench_serving_block_bookkeeping(fakes, monkeypatch, tmp_path):
+    """bench.py's serving block on the stand-ins: events, stalled jobs, and the
+    plain comparison (every job's events at its class's plain rate, plus the
+    stall window for each stalled job, which a plain run needs as well)."""
+    import bench
+
+    def plain_sim(cfg, output_dir=None):
+        s = FakeSim(cfg)
+        s.stats = {"thermal_events": 0}
+        s.t0 = 0
+
+        def run_simulation(*a, max_events=0, **k):
+            s.stats["thermal_events"] += max_events
+
+        def set_profiling(on):
+            s.t0 = s.stats["thermal_events"]
+
+        s.run_simulation, s.set_profiling = run_simulation, set_profiling
+        s.profile = lambda: {"run_ms": 0.5 * (s.stats["thermal_events"] - s.t0)}  # 2000 steps/s
+        return s
+
+    made = []
+    real_serve_jobs = workloads.serve_jobs
+
+    def serve_jobs(*a, **k):
+        jobs = real_serve_jobs(*a, **k)
+        made.extend(jobs)
+        fakes.add(id(jobs[2][1]))  # the third job never gets a thermal event
+        return jobs
+
+    monkeypatch.setattr(workloads, "serve_jobs", serve_jobs)
+    srv_from_config = G.from_config
+    # the serving loop builds with the stand-in above; the plain measurement afterwards
+    # uses plain_sim (from_config is looked up at each call)
+    calls = {"n": 0}
+
+    def from_config(cfg, output_dir=None):
+        calls["n"] += 1
+        return srv_from_config(cfg) if calls["n"] <= len(made) else plain_sim(cfg)
+
+    monkeypatch.setattr(G, "from_config", from_config)
+    monkeypatch.setattr(G, "_build_on", lambda dev, cfg: from_config(cfg))
+    out = bench.serve_block(G, workloads, str(tmp_path), 6, (30, 40), [("2d", 32)], slice_seconds=0.05,
+                            plain_events=20, build_threads=2)
+    targets = [t for _, _, t in made]
+    assert out["jobs"] == 6 and out["stalled_jobs"] == 1 and out["terminated_jobs"] == 0
+    assert out["events"] == sum(targets) - targets[2]
+    assert out["plain_stall_budget_seconds"] == 5.0
+    assert out["plain_job_by_job_seconds"] == pytest.approx(out["events"] / 2000.0 + 5.0)
+    assert out["speedup_vs_plain"] > out["speedup_vs_plain_without_stall_budget"]
