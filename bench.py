@@ -82,7 +82,7 @@ class ClockSampler:
     def start(self):
         cmd = ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu",
                "--format=csv,noheader,nounits", "-lms", "200"]
         try:
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
@@ -106,22 +106,41 @@ class ClockSampler:
             self.proc.kill()
         if self._t:
             self._t.join(timeout=2)
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[3:7]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return summarize_clocks(self.lines)
+
+
+def summarize_clocks(lines):
+    """Clock summary of nvidia-smi sample lines (clocks.sm, clocks.max.sm,
+    power.draw, four event reasons, utilization.gpu): the median SM clock
+    under load (samples with the GPU at least half busy; the window also holds
+    host-side gaps, where an idle GPU lowers its clock), the median over all
+    samples, the largest max clock, and every event reason seen active."""
+    sm, busy, mx, reasons = [], [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in lines:
+        parts = [x.strip() for x in ln.split(",")]
+        if len(parts) < 7:
+            continue
+        try:
+            f = float(parts[0])
+            m = float(parts[1])
+        except ValueError:
+            continue
+        sm.append(f)
+        mx.append(m)
+        try:
+            if len(parts) > 7 and float(parts[7]) >= 50.0:
+                busy.append(f)
+        except ValueError:
+            pass
+        for n, v in zip(names, parts[3:7]):
+            if v.lower() == "active":
+                reasons.add(n)
+    load = busy if busy else sm
+    return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons), "samples": len(sm), "samples_under_load": len(busy),
+            "sm_mhz_all_samples": float(np.median(sm)) if sm else None,
+            "what": "median SM clock over samples with utilization >= 50 % (all samples if none)"}
 
 
 def _traffic(key: str):
